@@ -1,0 +1,210 @@
+/* coresg_b200.h -- C ABI of the B200 (sm_100a) engine for the CORE-SG hot path.
+ *
+ * The engine keeps a CORE-SG resident in HBM (padded points, the k_max-NN arrays,
+ * the bridge edges and the derived undirected edge list) and runs, on one GPU:
+ * Dynamic NN-Descent, core distances, mutual-reachability reweighting, the per-mpts
+ * MST extraction (plain and as one batched persistent sweep), and the anti-hub
+ * bridge selection.  Citations are path:line in the reference project
+ * (voidosama/Incremental-CORE-SG).
+ *
+ * Conventions
+ *   - Every function returns a cs_status; on failure cs_last_error(ctx) holds the
+ *     message (per context; cs_last_error(NULL) is the calling thread's last error,
+ *     for failures before a context exists).  Mirrors the bool + thread-local
+ *     last_error() of include/coresg/cuda_api.hpp:22-23 / cuda/cuda_runtime_api.cu:17-23.
+ *   - Plain pointers and sizes only.  "host" pointers are caller-owned host memory;
+ *     the engine copies through its own pinned staging.  Distances cross the
+ *     boundary in metric units (L2 distance, not squared), like nndescent_gpu.
+ *   - One CUDA stream per context; calls on one context are serialised by a
+ *     per-context mutex.  There is no CPU fallback: a device failure is an error.
+ *   - Out of device memory is CS_ERR_OOM, never a crash (src/cuda_backend.cpp:88-103
+ *     records OOM as a result; the caller decides what to do).
+ */
+#ifndef CORESG_B200_H
+#define CORESG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t cs_status;
+enum {
+    CS_OK = 0,
+    CS_ERR_INVALID = 1,     /* bad argument (null pointer, size, mpts > k_max, ...) */
+    CS_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    CS_ERR_OOM = 3,         /* device allocation failed */
+    CS_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out; the context stays usable */
+    CS_ERR_UNSUPPORTED = 5, /* metric / size the device path does not cover */
+    CS_ERR_STATE = 6        /* call out of order (e.g. extract before a graph is loaded) */
+};
+
+/* Metric codes, as coresg::cuda::MetricCode (include/coresg/cuda_api.hpp:30-33). */
+enum { CS_METRIC_L2 = 0, CS_METRIC_COSINE = 1 };
+
+/* Same layout as coresg::Edge (include/coresg/types.hpp:20-33): u < v, weight w. */
+typedef struct {
+    uint32_t u;
+    uint32_t v;
+    float w;
+} cs_edge;
+
+/* Same fields as coresg::cuda::NndConfig (include/coresg/cuda_api.hpp:35-46). */
+typedef struct {
+    uint32_t n;
+    uint32_t dim;
+    uint32_t stride; /* padded row length in floats (multiple of 8, dataset.hpp:21) */
+    uint32_t k;
+    uint32_t sample; /* smpN; sampled old neighbours capped at 3 * sample */
+    uint32_t iters;
+    uint64_t seed;
+    int32_t metric;
+    float delta;         /* stop when a round's updates <= delta * k * n */
+    int32_t random_fill; /* top up unfilled slots with random candidates first */
+} cs_nnd_config;
+
+typedef struct cs_ctx cs_ctx;
+typedef struct cs_graph cs_graph;
+
+/* ---- device and context (cuda/cuda_runtime_api.cu:25-79) ------------------- */
+
+/* Replaces coresg::cuda::device_count (include/coresg/cuda_api.hpp:48). */
+cs_status cs_device_count(int32_t* out_count);
+/* Replaces get_device_props + device_memory (include/coresg/cuda_api.hpp:49, :80). */
+cs_status cs_device_props(int32_t device, char* name, size_t name_len, size_t* total_mem,
+                          size_t* free_mem, int32_t* sm_count, int32_t* cc_major,
+                          int32_t* cc_minor);
+/* Replaces coresg::cuda::last_error (include/coresg/cuda_api.hpp:52). */
+const char* cs_last_error(const cs_ctx* ctx);
+
+/* A context binds one device and owns one stream plus cached device scratch.  The
+ * reference binds a device per call (cudaSetDevice in nndescent_gpu); a context is
+ * the per-slot state that src/cuda_backend.cpp keeps per JobScheduler thread. */
+cs_status cs_ctx_create(int32_t device, cs_ctx** out_ctx);
+void cs_ctx_destroy(cs_ctx* ctx);
+/* Release cached scratch (coresg::cuda::release_thread_cache, cuda_api.hpp:84;
+ * Backend::trim, backend.hpp:91). */
+cs_status cs_ctx_trim(cs_ctx* ctx);
+/* Number of engine kernel launches issued on this context so far. */
+uint64_t cs_ctx_launches(const cs_ctx* ctx);
+
+/* ---- the two device entry points the reference's CUDA backend binds -------- */
+
+/* Dynamic NN-Descent on host buffers, start to finish: upload, optional random
+ * fill, <= iters rounds with the delta stop rule, download.  Replaces
+ * coresg::cuda::nndescent_gpu (include/coresg/cuda_api.hpp:57-59,
+ * cuda/nndescent_kernels.cu:295-437).  ids/dists/flags are n*k, counts n; dists in
+ * metric units; out_updates may be NULL. */
+cs_status cs_nndescent(cs_ctx* ctx, const cs_nnd_config* cfg, const float* host_vectors,
+                       uint32_t* ids, float* dists, uint8_t* flags, uint32_t* counts,
+                       uint64_t* out_updates);
+
+/* Rows [r0, r1) of the m x m mutual-reachability matrix max(d(i,j), core_i, core_j),
+ * 0 on the diagonal.  Replaces coresg::cuda::mrd_block_gpu
+ * (include/coresg/cuda_api.hpp:62-65, cuda/mrd_kernels.cu:218-243). */
+cs_status cs_mrd_block(cs_ctx* ctx, const float* host_pts, size_t m, uint32_t dim,
+                       uint32_t stride, int32_t metric, const float* host_core, size_t r0,
+                       size_t r1, float* host_out);
+
+/* ---- resident CORE-SG -------------------------------------------------------- */
+
+/* An empty device-resident CORE-SG with the given dimensionality and k_max
+ * (CoreSG state of include/coresg/coresg.hpp:198-204). k_max <= 64. */
+cs_status cs_graph_create(cs_ctx* ctx, uint32_t dim, uint32_t k_max, int32_t metric,
+                          cs_graph** out_graph);
+void cs_graph_destroy(cs_graph* g);
+
+/* n rows of `dim` floats (row_stride floats apart) -> padded device rows
+ * (Dataset::append, include/coresg/dataset.hpp:55-68; cosine rows are normalised). */
+cs_status cs_graph_set_points(cs_graph* g, const float* rows, uint64_t n, uint32_t row_stride);
+/* Append further rows (CoreSG::insert's Dataset::append + KnnGraph::grow). */
+cs_status cs_graph_append_points(cs_graph* g, const float* rows, uint64_t count,
+                                 uint32_t row_stride);
+/* k-NN arrays in the KnnGraph layout (include/coresg/knn_graph.hpp:191-197): n*k ids
+ * (0xFFFFFFFF unfilled), n*k dists (+inf unfilled, ascending), n*k flags, n counts.
+ * flags may be NULL (all zero). */
+cs_status cs_graph_set_knn(cs_graph* g, const uint32_t* ids, const float* dists,
+                           const uint8_t* flags, const uint32_t* counts, uint64_t n);
+cs_status cs_graph_get_knn(cs_graph* g, uint32_t* ids, float* dists, uint8_t* flags,
+                           uint32_t* counts);
+/* Bridge ("missing") edges with base distances (CoreSG::missing_edges,
+ * include/coresg/coresg.hpp:155). */
+cs_status cs_graph_set_bridges(cs_graph* g, const cs_edge* edges, uint64_t m);
+cs_status cs_graph_get_bridges(cs_graph* g, cs_edge* out, uint64_t cap, uint64_t* out_count);
+/* n, k_max, dim, stride, undirected k-NN edge count (KnnGraph::undirected_edge_count,
+ * src/knn_graph.cpp:202-217), bridge count.  Any pointer may be NULL. */
+cs_status cs_graph_info(cs_graph* g, uint64_t* n, uint32_t* k_max, uint32_t* dim,
+                        uint32_t* stride, uint64_t* knn_edges, uint64_t* bridges);
+
+/* ---- build: NN-Descent on the resident points + bridges --------------------- */
+
+/* k-NN graph of the resident points by Dynamic NN-Descent (IncrementalKnn::build
+ * with one instance, src/incremental_knn.cpp:1003-1050 -> nndescent_gpu): random
+ * fill, <= iters rounds, delta stop.  sample/iters/seed/delta as NNDescentParams
+ * (include/coresg/nndescent.hpp:45-71).  out_updates, out_rounds may be NULL. */
+cs_status cs_knn_build(cs_graph* g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
+                       uint64_t* out_updates, uint32_t* out_rounds);
+
+/* Anti-hub bridges for the current k-NN graph, all on device: connectivity
+ * (src/connectivity.cpp:99-139), reverse degrees and scores (src/hubness.cpp:44-158,
+ * :302-352), selection with the per-component quota (:424-521), the MRD MST over the
+ * selected set stored with base distances (src/coresg.cpp:97-141) and the
+ * connectivity repair (src/coresg.cpp:171-258).  Replaces the bridges half of
+ * CoreSG::build/insert (src/coresg.cpp:487-516, :565-583) with the defaults of
+ * CoreSGParams/HubnessParams.  Results: the graph's bridge set; counts optional. */
+cs_status cs_select_bridges(cs_graph* g, uint64_t* out_selected, uint64_t* out_bridges,
+                            uint64_t* out_repair, uint32_t* out_knn_components);
+/* The selected anti-hubs of the last cs_select_bridges (HubnessIndex::selected). */
+cs_status cs_get_selected(cs_graph* g, uint32_t* out, uint64_t cap, uint64_t* out_count);
+
+/* ---- extraction (new: the reference runs all of this on the host) ------------ */
+
+/* Core distances for mpts (CoreSG::core_distances, src/coresg.cpp:68-70 ->
+ * KnnGraph::core_dist, include/coresg/knn_graph.hpp:157-163).  out: n floats. */
+cs_status cs_core_distances(cs_graph* g, uint32_t mpts, float* host_out);
+
+/* CoreSG::edges(mpts) (src/coresg.cpp:391-406): the undirected k-NN edges in the
+ * reference's enumeration order, reweighted by mrd_mpts, then the bridges.  Writes
+ * min(count, cap) edges; *out_count gets the full count. */
+cs_status cs_edges(cs_graph* g, uint32_t mpts, cs_edge* host_out, uint64_t cap,
+                   uint64_t* out_count);
+
+/* MST_mpts of the CORE-SG, the plain per-mpts path: edges(mpts) materialised on
+ * device, then Boruvka rounds driven from the host, one launch sequence per mpts.
+ * Same result as CoreSG::mst (src/coresg.cpp:408-410 -> mst_boruvka,
+ * src/mst.cpp:79-151): the unique minimum spanning forest under (weight bits, edge
+ * index).  Outputs (all optional): out_edges (n-1 cap) in ascending edge-index
+ * order, out_labels (n; dense, numbered by smallest node), edge count, component
+ * count, and the total weight as the correctly rounded exact sum. */
+cs_status cs_extract(cs_graph* g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_labels,
+                     uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
+
+/* The batched sweep: K MSTs (one per entry of mpts[]) from the one resident edge
+ * list, reweighted on the fly and solved by one persistent cooperative launch
+ * replayed from a CUDA graph (CoreSG::all_msts, src/coresg.cpp:412-417, which the
+ * reference runs as K independent extractions).  Per-MST results as cs_extract,
+ * packed: out_edges K*(n-1), out_labels K*n, and K-long count/weight arrays.  Any
+ * output may be NULL. */
+cs_status cs_extract_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
+                           uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
+                           double* out_weight);
+
+/* Sweep results kept on the device: runs the sweep and leaves the K trees in the
+ * graph's result buffers (no host copy); *out_ms (optional) gets the device time of
+ * the launch in milliseconds.  Fetch with cs_sweep_fetch. */
+cs_status cs_extract_sweep_device(cs_graph* g, const uint32_t* mpts, uint32_t K, float* out_ms);
+cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
+                         uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
+
+/* Sweep tuning knobs (group size = MSTs solved concurrently, block size); 0 picks
+ * the cached autotuned value. */
+cs_status cs_set_sweep_shape(cs_graph* g, uint32_t group, uint32_t block_threads);
+cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_group,
+                            uint32_t* out_block);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CORESG_B200_H */

@@ -1,0 +1,259 @@
+// Contexts, device query, error plumbing, device/pinned buffers and staging copies.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace csb {
+
+namespace {
+thread_local std::string t_error;
+}
+
+void set_thread_error(const std::string& m) { t_error = m; }
+const char* thread_error() { return t_error.c_str(); }
+
+void fail(cs_status s, const std::string& msg) { throw Error(s, msg); }
+
+void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    if (e == cudaSuccess) return;
+    const bool oom = e == cudaErrorMemoryAllocation;
+    std::string msg = std::string(what) + " -> " + cudaGetErrorString(e) + " (" + file + ":" +
+                      std::to_string(line) + ")";
+    if (!oom) cudaGetLastError();  // clear sticky-free errors so the context stays usable
+    throw Error(oom ? CS_ERR_OOM : CS_ERR_CUDA, msg);
+}
+
+void check_launch(Ctx& c, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fail(e == cudaErrorMemoryAllocation ? CS_ERR_OOM : CS_ERR_CUDA,
+             std::string(what) + ": launch failed: " + cudaGetErrorString(e));
+    }
+    (void)c;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void DevBuf::ensure(size_t nbytes) {
+    if (nbytes <= bytes && p) return;
+    release();
+    if (nbytes == 0) nbytes = 16;
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, nbytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CS_ERR_OOM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: " +
+                             cudaGetErrorString(e));
+    }
+    p = q;
+    bytes = nbytes;
+}
+
+void DevBuf::grow_keep(size_t nbytes, cudaStream_t s) {
+    if (nbytes <= bytes && p) return;
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, nbytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CS_ERR_OOM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: " +
+                             cudaGetErrorString(e));
+    }
+    if (p && bytes) {
+        CSB_CUDA(cudaMemcpyAsync(q, p, bytes, cudaMemcpyDeviceToDevice, s));
+        CSB_CUDA(cudaStreamSynchronize(s));
+    }
+    release();
+    p = q;
+    bytes = nbytes;
+}
+
+void PinnedBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void PinnedBuf::ensure(size_t nbytes) {
+    if (nbytes <= bytes && p) return;
+    release();
+    void* q = nullptr;
+    const cudaError_t e = cudaMallocHost(&q, std::max<size_t>(nbytes, 64));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CS_ERR_OOM, std::string("cudaMallocHost failed: ") + cudaGetErrorString(e));
+    }
+    p = q;
+    bytes = std::max<size_t>(nbytes, 64);
+}
+
+void Ctx::bind() const { CSB_CUDA(cudaSetDevice(device)); }
+
+void Ctx::sync() { CSB_CUDA(cudaStreamSynchronize(stream)); }
+
+/// Host -> device through pinned staging, in 64 MiB chunks so the staging stays
+/// bounded; two staging halves let the memcpy into one overlap the DMA of the other.
+void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return;
+    const size_t chunk = size_t(32) << 20;
+    PinnedBuf& st = c.pinned[0];
+    st.ensure(2 * std::min(bytes, chunk));
+    const size_t half = st.bytes / 2;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    CSB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CSB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    int slot = 0;
+    bool used[2] = {false, false};
+    for (size_t off = 0; off < bytes; off += half) {
+        const size_t b = std::min(half, bytes - off);
+        if (used[slot]) CSB_CUDA(cudaEventSynchronize(ev[slot]));
+        char* stage = static_cast<char*>(st.p) + slot * half;
+        std::memcpy(stage, static_cast<const char*>(src) + off, b);
+        CSB_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, stage, b, cudaMemcpyHostToDevice, c.stream));
+        CSB_CUDA(cudaEventRecord(ev[slot], c.stream));
+        used[slot] = true;
+        slot ^= 1;
+    }
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+}
+
+void copy_d2h(Ctx& c, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return;
+    const size_t chunk = size_t(32) << 20;
+    PinnedBuf& st = c.pinned[1];
+    st.ensure(std::min(bytes, chunk));
+    for (size_t off = 0; off < bytes; off += st.bytes) {
+        const size_t b = std::min(st.bytes, bytes - off);
+        CSB_CUDA(cudaMemcpyAsync(st.p, static_cast<const char*>(src) + off, b, cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        std::memcpy(static_cast<char*>(dst) + off, st.p, b);
+    }
+}
+
+}  // namespace csb
+
+using namespace csb;
+
+extern "C" {
+
+cs_status cs_device_count(int32_t* out) {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (out) *out = 0;
+        set_thread_error(std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+        return (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? CS_OK : CS_ERR_CUDA;
+    }
+    if (out) *out = n;
+    return CS_OK;
+}
+
+cs_status cs_device_props(int32_t device, char* name, size_t name_len, size_t* total_mem,
+                          size_t* free_mem, int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor) {
+    try {
+        cudaDeviceProp p;
+        CSB_CUDA(cudaGetDeviceProperties(&p, device));
+        if (name && name_len) {
+            std::strncpy(name, p.name, name_len - 1);
+            name[name_len - 1] = 0;
+        }
+        if (total_mem) *total_mem = p.totalGlobalMem;
+        if (sm_count) *sm_count = p.multiProcessorCount;
+        if (cc_major) *cc_major = p.major;
+        if (cc_minor) *cc_minor = p.minor;
+        if (free_mem) {
+            int prev = 0;
+            CSB_CUDA(cudaGetDevice(&prev));
+            CSB_CUDA(cudaSetDevice(device));
+            size_t f = 0, t = 0;
+            CSB_CUDA(cudaMemGetInfo(&f, &t));
+            *free_mem = f;
+            CSB_CUDA(cudaSetDevice(prev));
+        }
+        return CS_OK;
+    } catch (const Error& e) {
+        set_thread_error(e.what());
+        return e.status;
+    }
+}
+
+const char* cs_last_error(const cs_ctx* ctx) {
+    const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
+    if (!c) return thread_error();
+    return c->last_error.c_str();
+}
+
+cs_status cs_ctx_create(int32_t device, cs_ctx** out) {
+    if (!out) {
+        set_thread_error("cs_ctx_create: null output");
+        return CS_ERR_INVALID;
+    }
+    *out = nullptr;
+    Ctx* c = new Ctx();
+    try {
+        c->device = device;
+        CSB_CUDA(cudaSetDevice(device));
+        cudaDeviceProp p;
+        CSB_CUDA(cudaGetDeviceProperties(&p, device));
+        c->sm_count = p.multiProcessorCount;
+        c->cc_major = p.major;
+        c->cc_minor = p.minor;
+        if (p.major < 10) {
+            fail(CS_ERR_UNSUPPORTED, "device is sm_" + std::to_string(p.major) +
+                                         std::to_string(p.minor) +
+                                         "; this library is built for sm_100a only");
+        }
+        CSB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->status.ensure(64);
+        CSB_CUDA(cudaMemsetAsync(c->status.p, 0, 64, c->stream));
+        CSB_CUDA(cudaStreamSynchronize(c->stream));
+        *out = reinterpret_cast<cs_ctx*>(c);
+        return CS_OK;
+    } catch (const Error& e) {
+        set_thread_error(e.what());
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return e.status;
+    }
+}
+
+void cs_ctx_destroy(cs_ctx* ctx) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return;
+    {
+        std::lock_guard<std::recursive_mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        for (auto& b : c->scratch) b.release();
+        c->status.release();
+        for (auto& b : c->pinned) b.release();
+        cudaStreamDestroy(c->stream);
+        c->stream = nullptr;
+    }
+    delete c;
+}
+
+cs_status cs_ctx_trim(cs_ctx* ctx) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    return guarded(c, [&] {
+        c->sync();
+        for (auto& b : c->scratch) b.release();
+        for (auto& b : c->pinned) b.release();
+    });
+}
+
+uint64_t cs_ctx_launches(const cs_ctx* ctx) {
+    const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
+    return c ? c->launches : 0;
+}
+
+}  // extern "C"

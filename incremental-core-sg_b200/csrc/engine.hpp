@@ -1,0 +1,196 @@
+// Host-side internals of the B200 CORE-SG engine: contexts, resident graphs,
+// device buffers and error plumbing shared by the .cu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "coresg_b200.h"
+
+namespace csb {
+
+// ---- errors -------------------------------------------------------------------
+
+struct Error : std::runtime_error {
+    cs_status status;
+    Error(cs_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] void fail(cs_status s, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define CSB_CUDA(expr) ::csb::check_cuda((expr), #expr, __FILE__, __LINE__)
+#define CSB_REQUIRE(cond, msg)                                   \
+    do {                                                         \
+        if (!(cond)) ::csb::fail(CS_ERR_INVALID, (msg));         \
+    } while (0)
+
+void set_thread_error(const std::string& m);
+const char* thread_error();
+
+// ---- device memory ----------------------------------------------------------
+
+/// Owning device allocation that only grows.  cudaMalloc failures surface as
+/// CS_ERR_OOM.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release();
+    void ensure(size_t nbytes);  // contents not preserved when it grows
+    void grow_keep(size_t nbytes, cudaStream_t s);  // contents preserved
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+/// Pinned host staging that only grows.
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { release(); }
+    void release();
+    void ensure(size_t nbytes);
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// ---- context ------------------------------------------------------------------
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    int cc_major = 0, cc_minor = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    std::string last_error;
+    uint64_t launches = 0;  // engine kernel launches issued
+    DevBuf scratch[8];      // per-call scratch, reused across calls
+    PinnedBuf pinned[2];
+    DevBuf status;          // device error word(s) written by bounded waits
+    void bind() const;      // cudaSetDevice(device)
+    void sync();            // stream synchronise + error check
+};
+
+// ---- resident CORE-SG -------------------------------------------------------------
+
+struct SweepPlan;  // mst.cu
+
+struct Graph {
+    Ctx* ctx = nullptr;
+    uint32_t dim = 0, k = 0, stride = 0;
+    int metric = CS_METRIC_L2;
+    uint64_t n = 0;       // nodes with points
+    uint64_t knn_n = 0;   // nodes with k-NN arrays (== n once set)
+    uint64_t cap_n = 0;   // allocated node capacity
+
+    DevBuf pts;     // float [cap_n][stride]
+    DevBuf ids;     // u32  [cap_n][k]
+    DevBuf dists;   // f32  [cap_n][k]
+    DevBuf flags;   // u8   [cap_n][k]
+    DevBuf counts;  // u32  [cap_n]
+    DevBuf bridges; // cs_edge [nb]
+    uint64_t nb = 0;
+    uint64_t n_repair = 0;
+
+    // Derived undirected edge list (base weights), in the reference order:
+    // k-NN edges node-major (src/knn_graph.cpp:132-200), then the bridges.
+    bool edges_valid = false;
+    uint64_t e_knn = 0, e_total = 0;
+    DevBuf eu, ev, ew;    // SoA u32/u32/f32 [e_total]
+    DevBuf node_off;      // u32 [n+1] offsets of each node's emitted edges
+
+    // Hubness selection of the last cs_select_bridges.
+    std::vector<uint32_t> selected;
+
+    // Batched sweep state (mst.cu).
+    SweepPlan* plan = nullptr;
+    uint32_t sweep_group = 0, sweep_block = 0;  // 0 = autotuned/cached
+
+    ~Graph();
+    void invalidate_edges() { edges_valid = false; }
+    void ensure_capacity(uint64_t need, bool keep);
+};
+
+// ---- module entry points (implemented in the .cu files) ----------------------------
+
+// graph.cu
+void graph_build_edges(Graph& g);  // cached base edge list (no-op when valid)
+uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf& u, DevBuf& v,
+                                 DevBuf& w, DevBuf& core_out, DevBuf& tmp_mask, DevBuf& tmp_cnt,
+                                 DevBuf& tmp_off);
+void launch_core(const Graph& g, uint32_t mpts, float* core, cudaStream_t s);
+
+// mst.cu
+struct MstHost {
+    uint64_t nedges = 0;
+    uint32_t ncomp = 0;
+    double weight = 0.0;
+};
+void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
+void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms);
+void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
+void sweep_free(SweepPlan* p);
+double exact_sum_from_bins(const uint64_t* bins256);
+
+// knn.cu
+void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
+                 bool random_fill, uint64_t* out_updates, uint32_t* out_rounds);
+
+// bridges.cu
+void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
+                    uint32_t* out_components);
+void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metric,
+              const float* d_core, uint32_t r0, uint32_t r1, float* d_out);
+
+// scan.cu
+/// Exclusive prefix sum of n u32 values into out (n+1 entries; out[n] = total).
+void scan_u32(Ctx& c, const uint32_t* in, uint32_t* out, uint64_t n);
+
+// host <-> device through the context's pinned staging (context.cu)
+void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes);
+void copy_d2h(Ctx& c, void* dst, const void* src, size_t bytes);
+
+/// Run `f` for a C entry point: lock the context, bind its device, translate
+/// exceptions into a status plus the context's last error.
+template <typename F>
+cs_status guarded(Ctx* c, F&& f) {
+    if (!c) {
+        set_thread_error("null context or handle");
+        return CS_ERR_INVALID;
+    }
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    try {
+        c->bind();
+        f();
+        return CS_OK;
+    } catch (const Error& e) {
+        c->last_error = e.what();
+        set_thread_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        c->last_error = "host allocation failed";
+        set_thread_error(c->last_error);
+        return CS_ERR_OOM;
+    } catch (const std::exception& e) {
+        c->last_error = e.what();
+        set_thread_error(e.what());
+        return CS_ERR_INVALID;
+    }
+}
+
+// launch bookkeeping
+inline void count_launch(Ctx& c, uint64_t n = 1) { c.launches += n; }
+void check_launch(Ctx& c, const char* what);
+
+}  // namespace csb

@@ -1,0 +1,1003 @@
+// MST_mpts extraction over the resident CORE-SG edge list.
+//
+// Result contract (both paths): the unique minimum spanning forest under the total
+// order (weight bits, edge index) -- the order the reference's Boruvka selects by
+// (pack_edge, src/mst.cpp:19-24; mst_boruvka :79-151) -- so the tree is the
+// reference's tree edge for edge.  Components are labelled densely in order of their
+// smallest node (UnionFind::labels, mst.cpp:48-59).  The weight is the correctly
+// rounded exact sum of the tree weights (per-exponent integer bins), which is a
+// function of the weight multiset alone.
+//
+// Boruvka round r, per MST:
+//   A  every live edge i (implicit "all edges" in rounds 0-1, else the worklist)
+//      finds the roots of its endpoints; if they differ it atomicMin's the packed
+//      key (w' bits << 32 | i) into best[root] of both, appends itself to the next
+//      worklist, and the first toucher of a root appends the root to `touched`.
+//   B  every touched root takes its best edge, marks it in the tree bitmap (the
+//      first marker adds its weight and unites the endpoints; a doubly chosen edge
+//      is counted once) and resets best[root].
+// Roots are linked larger-under-smaller, so after the last round find(v) is the
+// smallest node of v's component, which is what the dense labelling needs.
+//
+// Plain path (cs_extract): edges(mpts) materialised per call exactly as
+// CoreSG::edges does, then one kernel per phase with a host read of the counters
+// after every phase A (the reference's round loop, moved to the device).
+// Batched path (cs_extract_sweep): the cached base edge list is reweighted on the
+// fly for every mpts; all K MSTs run inside ONE cooperative persistent kernel,
+// G MSTs at a time (their union-find state stays L2-resident), with a bounded grid
+// barrier between phases; the whole sequence is captured once in a CUDA graph.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace csb {
+
+struct MstView {
+    uint32_t* parent;
+    unsigned long long* best;
+    uint32_t* touched;
+    uint32_t* wl0;
+    uint32_t* wl1;
+    uint32_t* bitmap;
+    unsigned long long* bins;
+    uint32_t* ctr;  // [0] wc0 [1] wc1 [2] tc0 [3] tc1
+    const float* core;
+};
+
+namespace {
+
+constexpr int kMaxRounds = 64;
+constexpr int kThreads = 256;
+constexpr int kTileWords = 2048;  // compaction tile: 256 threads x 8 words
+constexpr uint64_t kBarrierLimitNs = 2000000000ull;
+
+inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
+    uint64_t b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > (1u << 30)) b = 1u << 30;
+    return static_cast<unsigned>(b);
+}
+
+__device__ __forceinline__ uint32_t bin_of(uint32_t bits) {
+    const uint32_t e = (bits >> 23) & 0xFFu;
+    return e ? e : 1u;
+}
+__device__ __forceinline__ uint32_t mant_of(uint32_t bits) {
+    const uint32_t e = (bits >> 23) & 0xFFu;
+    return (bits & 0x7FFFFFu) | (e ? 0x800000u : 0u);
+}
+
+/// Phase A for one edge.  Must be called by all 32 lanes of a warp together
+/// (`valid` false for padding lanes).
+template <bool kReweight>
+__device__ __forceinline__ void edge_step(const MstView& m, uint32_t i, bool valid, uint32_t u,
+                                          uint32_t v, float w, uint32_t n, int r, bool write_wl) {
+    bool live = false, t1 = false, t2 = false;
+    uint32_t cu = 0, cv = 0;
+    if (valid && u < n && v < n) {
+        if (kReweight) w = max_ref(w, max_ref(__ldg(m.core + u), __ldg(m.core + v)));
+        cu = uf_find(m.parent, u);
+        cv = uf_find(m.parent, v);
+        live = cu != cv;
+        if (live) {
+            const unsigned long long key = pack_key(w, i);
+            t1 = atomicMin(m.best + cu, key) == kNoKey;
+            t2 = atomicMin(m.best + cv, key) == kNoKey;
+        }
+    }
+    if (write_wl) {
+        const int o = (r + 1) & 1;
+        const uint32_t slot = warp_append(live, m.ctr + o);
+        if (live) (o ? m.wl1 : m.wl0)[slot] = i;
+    }
+    uint32_t* tc = m.ctr + 2 + (r & 1);
+    const uint32_t s1 = warp_append(t1, tc);
+    if (t1) m.touched[s1] = cu;
+    const uint32_t s2 = warp_append(t2, tc);
+    if (t2) m.touched[s2] = cv;
+}
+
+/// Phase B for one touched root.
+__device__ __forceinline__ void root_step(const MstView& m, uint32_t c, const uint32_t* __restrict__ eu,
+                                          const uint32_t* __restrict__ ev, unsigned long long* sbins,
+                                          int* status) {
+    const unsigned long long key = __ldcg(m.best + c);
+    m.best[c] = kNoKey;
+    if (key == kNoKey) return;
+    const uint32_t i = static_cast<uint32_t>(key);
+    const uint32_t bits = static_cast<uint32_t>(key >> 32);
+    const uint32_t bit = 1u << (i & 31u);
+    const uint32_t old = atomicOr(m.bitmap + (i >> 5), bit);
+    if (!(old & bit)) {
+        atomicAdd(sbins + bin_of(bits), static_cast<unsigned long long>(mant_of(bits)));
+        uf_unite(m.parent, __ldg(eu + i), __ldg(ev + i), status);
+    }
+}
+
+__device__ __forceinline__ void flush_bins(unsigned long long* sbins, unsigned long long* gbins) {
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+        const unsigned long long x = sbins[b];
+        if (x) {
+            atomicAdd(gbins + b, x);
+            sbins[b] = 0;
+        }
+    }
+    __syncthreads();
+}
+
+// ---- plain path kernels -------------------------------------------------------------
+
+__global__ void k_iota(uint32_t* __restrict__ parent, uint64_t total, uint32_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < total) parent[i] = static_cast<uint32_t>(i % n);
+}
+
+__global__ void k_phase_a(MstView m, const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev,
+                          const float* __restrict__ ew, uint32_t n, uint32_t count, int r) {
+    const bool implicit = r <= 1;
+    const uint64_t padded = (static_cast<uint64_t>(count) + 31) & ~31ull;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint32_t* in = (r & 1) ? m.wl1 : m.wl0;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < padded; t += stride) {
+        const bool valid = t < count;
+        uint32_t i = 0, u = 0, v = 0;
+        float w = 0.0f;
+        if (valid) {
+            i = implicit ? static_cast<uint32_t>(t) : in[t];
+            u = __ldg(eu + i);
+            v = __ldg(ev + i);
+            w = __ldg(ew + i);
+        }
+        edge_step<false>(m, i, valid, u, v, w, n, r, r >= 1);
+    }
+}
+
+__global__ void k_phase_b(MstView m, const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev,
+                          uint32_t count, int* status) {
+    __shared__ unsigned long long sbins[256];
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) sbins[b] = 0;
+    __syncthreads();
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < count; t += stride) {
+        root_step(m, m.touched[t], eu, ev, sbins, status);
+    }
+    flush_bins(sbins, m.bins);
+}
+
+// ---- the batched persistent kernel ------------------------------------------------------
+
+struct SweepArgs {
+    uint32_t n, E, K, G, W;
+    const uint32_t* eu;
+    const uint32_t* ev;
+    const float* ew;
+    const float* core;          // K*n
+    uint32_t* parent;           // K*n
+    unsigned long long* best;   // G*n
+    uint32_t* touched;          // G*n
+    uint32_t* wl;               // G*2*E
+    uint32_t* bitmap;           // K*W
+    unsigned long long* bins;   // K*256
+    uint32_t* ctr;              // G*8
+    unsigned* bar;              // [0] count, [1] generation
+    int* status;
+    uint64_t limit_ns;
+};
+
+__device__ __forceinline__ MstView view_of(const SweepArgs& a, uint32_t slot, uint32_t j) {
+    MstView m;
+    m.parent = a.parent + static_cast<uint64_t>(j) * a.n;
+    m.best = a.best + static_cast<uint64_t>(slot) * a.n;
+    m.touched = a.touched + static_cast<uint64_t>(slot) * a.n;
+    m.wl0 = a.wl + static_cast<uint64_t>(slot) * 2 * a.E;
+    m.wl1 = m.wl0 + a.E;
+    m.bitmap = a.bitmap + static_cast<uint64_t>(j) * a.W;
+    m.bins = a.bins + static_cast<uint64_t>(j) * 256;
+    m.ctr = a.ctr + slot * 8;
+    m.core = a.core + static_cast<uint64_t>(j) * a.n;
+    return m;
+}
+
+__global__ void __launch_bounds__(512) k_sweep(SweepArgs a) {
+    __shared__ unsigned long long sbins[256];
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) sbins[b] = 0;
+    const uint64_t gtid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t gstride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+
+    for (uint32_t g0 = 0; g0 < a.K; g0 += a.G) {
+        const uint32_t slots = min(a.G, a.K - g0);
+        // -- group init: identity parents, zero counters (best[] is all-empty
+        //    between groups: every touched root is reset in its phase B).
+        const uint64_t pn = static_cast<uint64_t>(slots) * a.n;
+        for (uint64_t t = gtid; t < pn; t += gstride) {
+            a.parent[static_cast<uint64_t>(g0) * a.n + t] = static_cast<uint32_t>(t % a.n);
+        }
+        if (blockIdx.x == 0 && threadIdx.x < slots * 8) a.ctr[threadIdx.x] = 0;
+        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+
+        uint32_t active = (slots >= 32) ? 0xFFFFFFFFu : ((1u << slots) - 1u);
+        int r = 0;
+        for (; r < kMaxRounds; ++r) {
+            // ---- phase A
+            if (r <= 1) {
+                const uint64_t padded = (static_cast<uint64_t>(a.E) + 31) & ~31ull;
+                for (uint64_t t = gtid; t < padded; t += gstride) {
+                    const bool valid = t < a.E;
+                    uint32_t u = 0, v = 0;
+                    float w = 0.0f;
+                    if (valid) {
+                        u = __ldg(a.eu + t);
+                        v = __ldg(a.ev + t);
+                        w = __ldg(a.ew + t);
+                    }
+                    for (uint32_t s = 0; s < slots; ++s) {
+                        if (!(active >> s & 1u)) continue;
+                        edge_step<true>(view_of(a, s, g0 + s), static_cast<uint32_t>(t), valid, u, v, w,
+                                        a.n, r, r == 1);
+                    }
+                }
+            } else {
+                for (uint32_t s = 0; s < slots; ++s) {
+                    if (!(active >> s & 1u)) continue;
+                    const MstView m = view_of(a, s, g0 + s);
+                    const uint32_t cnt = __ldcg(m.ctr + (r & 1));
+                    const uint32_t* in = (r & 1) ? m.wl1 : m.wl0;
+                    const uint64_t padded = (static_cast<uint64_t>(cnt) + 31) & ~31ull;
+                    for (uint64_t t = gtid; t < padded; t += gstride) {
+                        const bool valid = t < cnt;
+                        uint32_t i = 0, u = 0, v = 0;
+                        float w = 0.0f;
+                        if (valid) {
+                            i = __ldcg(in + t);
+                            u = __ldg(a.eu + i);
+                            v = __ldg(a.ev + i);
+                            w = __ldg(a.ew + i);
+                        }
+                        edge_step<true>(m, i, valid, u, v, w, a.n, r, true);
+                    }
+                }
+            }
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+
+            // ---- termination: an MST with no live edge left is done
+            for (uint32_t s = 0; s < slots; ++s) {
+                if (!(active >> s & 1u)) continue;
+                if (__ldcg(a.ctr + s * 8 + 2 + (r & 1)) == 0) active &= ~(1u << s);
+            }
+            if (active == 0) break;
+
+            // ---- phase B
+            for (uint32_t s = 0; s < slots; ++s) {
+                if (!(active >> s & 1u)) continue;
+                const MstView m = view_of(a, s, g0 + s);
+                const uint32_t tcnt = __ldcg(m.ctr + 2 + (r & 1));
+                for (uint64_t t = gtid; t < tcnt; t += gstride) {
+                    root_step(m, __ldcg(m.touched + t), a.eu, a.ev, sbins, a.status);
+                }
+                flush_bins(sbins, m.bins);
+            }
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                for (uint32_t s = 0; s < slots; ++s) {
+                    a.ctr[s * 8 + (r & 1)] = 0;            // next round's append target
+                    a.ctr[s * 8 + 2 + ((r + 1) & 1)] = 0;  // next round's touched count
+                }
+            }
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        }
+        if (r == kMaxRounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusRoundLimit);
+    }
+}
+
+/// Core tables of K mpts values: core[j][v], one dist row read per node.
+__global__ void k_core_multi(const float* __restrict__ dists, const uint32_t* __restrict__ counts,
+                             uint32_t n, uint32_t k, const uint32_t* __restrict__ mpts, uint32_t K,
+                             float* __restrict__ core) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    for (uint32_t j = 0; j < K; ++j) core[static_cast<uint64_t>(j) * n + v] = core_of(dists, counts, k, v, mpts[j]);
+}
+
+// ---- labels: dense, numbered by smallest node -------------------------------------------
+
+__device__ __forceinline__ uint32_t block_prefix_flags(bool f, uint32_t* total) {
+    __shared__ uint32_t wsum[32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, f);
+    const uint32_t in_warp = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) wsum[warp] = __popc(m);
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+    const unsigned nw = blockDim.x >> 5;
+    for (unsigned w = 0; w < nw; ++w) {
+        if (w < warp) before += wsum[w];
+        all += wsum[w];
+    }
+    __syncthreads();
+    if (total) *total = all;
+    return before + in_warp;
+}
+
+__global__ void k_label_roots(uint32_t* __restrict__ parent_all, uint32_t n, uint32_t* __restrict__ lab_all,
+                              uint32_t* __restrict__ bc, uint32_t nb) {
+    const uint32_t j = blockIdx.y;
+    uint32_t* parent = parent_all + static_cast<uint64_t>(j) * n;
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    bool root = false;
+    if (v < n) {
+        const uint32_t r = uf_find(parent, v);
+        lab_all[static_cast<uint64_t>(j) * n + v] = r;
+        root = r == v;
+    }
+    uint32_t total;
+    block_prefix_flags(root, &total);
+    if (threadIdx.x == 0) bc[static_cast<uint64_t>(j) * nb + blockIdx.x] = total;
+}
+
+__global__ void k_label_dense(const uint32_t* __restrict__ parent_all, uint32_t n, uint32_t* __restrict__ lab_all,
+                              const uint32_t* __restrict__ bc, uint32_t nb) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool root = v < n && __ldcg(parent_all + static_cast<uint64_t>(j) * n + v) == v;
+    const uint32_t pre = block_prefix_flags(root, nullptr);
+    if (root) lab_all[static_cast<uint64_t>(j) * n + v] = bc[static_cast<uint64_t>(j) * nb + blockIdx.x] + pre;
+}
+
+__global__ void k_label_fill(const uint32_t* __restrict__ parent_all, uint32_t n, uint32_t* __restrict__ lab_all) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const uint64_t base = static_cast<uint64_t>(j) * n;
+    if (__ldcg(parent_all + base + v) != v) lab_all[base + v] = lab_all[base + lab_all[base + v]];
+}
+
+/// Exclusive scan of `nt` u32 tile counts per MST (one block per MST); total -> tot[j].
+__global__ void k_scan_tiles(uint32_t* __restrict__ tiles, uint32_t nt, unsigned long long* __restrict__ tot) {
+    const uint32_t j = blockIdx.x;
+    uint32_t* t = tiles + static_cast<uint64_t>(j) * nt;
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t base = 0; base < nt; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t x = i < nt ? t[i] : 0u;
+        uint32_t incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= static_cast<unsigned>(o)) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (unsigned w = 0; w < nw; ++w) {
+            if (w < warp) before += wsum[w];
+            all += wsum[w];
+        }
+        if (i < nt) t[i] = carry + before + incl - x;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += all;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tot[j] = carry;
+}
+
+// ---- tree bitmap -> edge list (ascending edge index) -----------------------------------
+
+__global__ void k_bits_tiles(const uint32_t* __restrict__ bitmap, uint32_t W, uint32_t nt,
+                             uint32_t* __restrict__ tiles) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t* bm = bitmap + static_cast<uint64_t>(j) * W;
+    uint32_t s = 0;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTileWords + threadIdx.x * 8ull;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        if (base + t < W) s += __popc(__ldcg(bm + base + t));
+    }
+    __shared__ uint32_t red[kThreads];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tiles[static_cast<uint64_t>(j) * nt + blockIdx.x] = red[0];
+}
+
+__global__ void k_bits_emit(const uint32_t* __restrict__ bitmap, uint32_t W, uint32_t nt,
+                            const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ eu,
+                            const uint32_t* __restrict__ ev, const float* __restrict__ ew,
+                            const float* __restrict__ core, uint32_t n, uint64_t cap,
+                            cs_edge* __restrict__ out, int* status) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t* bm = bitmap + static_cast<uint64_t>(j) * W;
+    const float* cj = core ? core + static_cast<uint64_t>(j) * n : nullptr;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTileWords + threadIdx.x * 8ull;
+    uint32_t words[8];
+    uint32_t s = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        words[t] = (base + t < W) ? __ldcg(bm + base + t) : 0u;
+        s += __popc(words[t]);
+    }
+    // block exclusive scan of s
+    __shared__ uint32_t wsum[32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= static_cast<unsigned>(o)) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (unsigned w = 0; w < nw && w < warp; ++w) before += wsum[w];
+    uint64_t pos = tiles[static_cast<uint64_t>(j) * nt + blockIdx.x] + before + incl - s;
+    cs_edge* o = out + static_cast<uint64_t>(j) * cap;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        uint32_t bits = words[t];
+        while (bits) {
+            const uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const uint32_t i = static_cast<uint32_t>((base + t) * 32 + b);
+            const uint32_t u = eu[i], v = ev[i];
+            float w = ew[i];
+            if (cj) w = max_ref(w, max_ref(cj[u], cj[v]));
+            if (pos < cap) {
+                cs_edge e;
+                e.u = u;
+                e.v = v;
+                e.w = w;
+                o[pos] = e;
+            } else {
+                atomicOr(status, kStatusCapacity);
+            }
+            ++pos;
+        }
+    }
+}
+
+}  // namespace
+
+// ============================================================================
+// exact weight from per-exponent bins
+// ============================================================================
+
+/// Correctly rounded double of sum_e bins[e] * 2^(e-150) (bins hold 24-bit
+/// mantissas with the hidden bit; bin 255 non-empty means an infinite weight).
+double exact_sum_from_bins(const uint64_t* bins) {
+    if (bins[255]) return INFINITY;
+    constexpr int L = 12;  // 384 bits; bins[e] (< 2^64) lands at bit e-1
+    uint64_t limb[L] = {0};
+    for (int e = 1; e < 255; ++e) {
+        uint64_t x = bins[e];
+        if (!x) continue;
+        const int sh = e - 1;
+        int li = sh / 32;
+        const int off = sh % 32;
+        unsigned __int128 y = static_cast<unsigned __int128>(x) << off;
+        while (y && li < L) {
+            const unsigned __int128 s = static_cast<unsigned __int128>(limb[li]) + static_cast<uint64_t>(y & 0xFFFFFFFFu);
+            limb[li] = static_cast<uint64_t>(s & 0xFFFFFFFFu);
+            y = (y >> 32) + (s >> 32);
+            ++li;
+        }
+    }
+    int top = -1;
+    for (int li = L - 1; li >= 0 && top < 0; --li) {
+        if (!limb[li]) continue;
+        for (int b = 31; b >= 0; --b) {
+            if (limb[li] >> b & 1u) {
+                top = li * 32 + b;
+                break;
+            }
+        }
+    }
+    if (top < 0) return 0.0;
+    auto bit = [&](int p) -> unsigned { return p < 0 ? 0u : static_cast<unsigned>((limb[p / 32] >> (p % 32)) & 1u); };
+    uint64_t mant = 0;
+    const int low = top - 52;
+    for (int p = top; p >= low && p >= 0; --p) mant = (mant << 1) | bit(p);
+    if (low <= 0) return std::ldexp(static_cast<double>(mant), -149);
+    const unsigned rb = bit(low - 1);
+    unsigned sticky = 0;
+    for (int p = low - 2; p >= 0 && !sticky; --p) sticky |= bit(p);
+    if (rb && (sticky || (mant & 1u))) ++mant;
+    return std::ldexp(static_cast<double>(mant), low - 149);
+}
+
+// ============================================================================
+// shared finishing: labels + compaction for K MSTs
+// ============================================================================
+
+namespace {
+
+void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_t* lab_all,
+                   uint32_t* bc, unsigned long long* ncomp) {
+    const uint32_t nb = blocks_for(n);
+    dim3 grid(nb, K);
+    k_label_roots<<<grid, kThreads, 0, c.stream>>>(parent_all, n, lab_all, bc, nb);
+    k_scan_tiles<<<K, 1024, 0, c.stream>>>(bc, nb, ncomp);
+    k_label_dense<<<grid, kThreads, 0, c.stream>>>(parent_all, n, lab_all, bc, nb);
+    k_label_fill<<<grid, kThreads, 0, c.stream>>>(parent_all, n, lab_all);
+    count_launch(c, 4);
+}
+
+void launch_compact(Ctx& c, const uint32_t* bitmap, uint32_t W, uint32_t K, uint32_t* tiles,
+                    unsigned long long* nedges, const uint32_t* eu, const uint32_t* ev, const float* ew,
+                    const float* core, uint32_t n, uint64_t cap, cs_edge* out, int* status) {
+    const uint32_t nt = std::max<uint32_t>(1, (W + kTileWords - 1) / kTileWords);
+    dim3 grid(nt, K);
+    k_bits_tiles<<<grid, kThreads, 0, c.stream>>>(bitmap, W, nt, tiles);
+    k_scan_tiles<<<K, 1024, 0, c.stream>>>(tiles, nt, nedges);
+    k_bits_emit<<<grid, kThreads, 0, c.stream>>>(bitmap, W, nt, tiles, eu, ev, ew, core, n, cap, out, status);
+    count_launch(c, 3);
+}
+
+void status_check(Ctx& c, const int* d_status) {
+    int st = 0;
+    CSB_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    if (st & kStatusBarrierTimeout) fail(CS_ERR_TIMEOUT, "MST sweep: a grid barrier wait ran out (device status 0x" + std::to_string(st) + ")");
+    if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "MST: a union retry loop ran out");
+    if (st & kStatusRoundLimit) fail(CS_ERR_TIMEOUT, "MST: Boruvka round limit reached");
+    if (st & kStatusCapacity) fail(CS_ERR_STATE, "MST: tree larger than n-1 edges (inconsistent state)");
+}
+
+}  // namespace
+
+// ============================================================================
+// plain per-mpts path
+// ============================================================================
+
+void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_labels, MstHost* res) {
+    Ctx& c = *g.ctx;
+    const uint32_t n = static_cast<uint32_t>(g.n);
+    if (mpts == 0) mpts = 1;
+    if (mpts > g.k) fail(CS_ERR_INVALID, "CoreSG::edges: mpts exceeds k_max");
+    // edges(mpts), materialised and reweighted (the reference rebuilds them per call)
+    DevBuf eu, ev, ew, core;
+    const uint64_t E = graph_materialize_edges(g, mpts, true, eu, ev, ew, core, c.scratch[0],
+                                               c.scratch[1], c.scratch[2]);
+    const uint32_t W = static_cast<uint32_t>((E + 31) / 32) + 1;
+    DevBuf parent, best, touched, wl, bitmap, bins, ctr, tiles, lab, outb;
+    parent.ensure(std::max<uint64_t>(n, 1) * 4);
+    best.ensure(std::max<uint64_t>(n, 1) * 8);
+    touched.ensure(std::max<uint64_t>(n, 1) * 4);
+    wl.ensure(std::max<uint64_t>(E, 1) * 8);
+    bitmap.ensure(static_cast<uint64_t>(W) * 4);
+    bins.ensure(256 * 8 + 64);
+    ctr.ensure(64);
+    const uint32_t nbl = blocks_for(n);
+    const uint32_t ntl = std::max<uint32_t>(1, (W + kTileWords - 1) / kTileWords);
+    tiles.ensure((static_cast<uint64_t>(nbl) + ntl + 2) * 4 + 64);
+    int* status = c.status.as<int>();
+    CSB_CUDA(cudaMemsetAsync(status, 0, 4, c.stream));
+    CSB_CUDA(cudaMemsetAsync(best.p, 0xFF, std::max<uint64_t>(n, 1) * 8, c.stream));
+    CSB_CUDA(cudaMemsetAsync(bitmap.p, 0, static_cast<uint64_t>(W) * 4, c.stream));
+    CSB_CUDA(cudaMemsetAsync(bins.p, 0, 256 * 8 + 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(ctr.p, 0, 64, c.stream));
+    if (n) {
+        k_iota<<<blocks_for(n), kThreads, 0, c.stream>>>(parent.as<uint32_t>(), n, n);
+        count_launch(c);
+    }
+    MstView m;
+    m.parent = parent.as<uint32_t>();
+    m.best = best.as<unsigned long long>();
+    m.touched = touched.as<uint32_t>();
+    m.wl0 = wl.as<uint32_t>();
+    m.wl1 = wl.as<uint32_t>() + std::max<uint64_t>(E, 1);
+    m.bitmap = bitmap.as<uint32_t>();
+    m.bins = bins.as<unsigned long long>();
+    m.ctr = ctr.as<uint32_t>();
+    m.core = nullptr;
+    const unsigned grid_cap = static_cast<unsigned>(c.sm_count) * 8u;
+    uint32_t in_count = static_cast<uint32_t>(E);
+    uint32_t hc[4];
+    int r = 0;
+    for (; r < kMaxRounds; ++r) {
+        if (r <= 1) in_count = static_cast<uint32_t>(E);
+        const unsigned gA = std::min<unsigned>(grid_cap, blocks_for(in_count));
+        k_phase_a<<<gA, kThreads, 0, c.stream>>>(m, eu.as<uint32_t>(), ev.as<uint32_t>(), ew.as<float>(),
+                                                  n, in_count, r);
+        count_launch(c);
+        check_launch(c, "boruvka phase A");
+        // the host reads the round's counters, as the reference's round loop does
+        CSB_CUDA(cudaMemcpyAsync(hc, m.ctr, sizeof(hc), cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        const uint32_t tcount = hc[2 + (r & 1)];
+        if (tcount == 0) break;
+        const unsigned gB = std::min<unsigned>(grid_cap, blocks_for(tcount));
+        k_phase_b<<<gB, kThreads, 0, c.stream>>>(m, eu.as<uint32_t>(), ev.as<uint32_t>(), tcount, status);
+        count_launch(c);
+        check_launch(c, "boruvka phase B");
+        in_count = hc[(r + 1) & 1];
+        CSB_CUDA(cudaMemsetAsync(m.ctr + (r & 1), 0, 4, c.stream));
+        CSB_CUDA(cudaMemsetAsync(m.ctr + 2 + ((r + 1) & 1), 0, 4, c.stream));
+    }
+    if (r == kMaxRounds) fail(CS_ERR_TIMEOUT, "MST: Boruvka round limit reached");
+
+    DevBuf counts;
+    counts.ensure(64);
+    unsigned long long* d_ncomp = counts.as<unsigned long long>();
+    unsigned long long* d_nedges = d_ncomp + 1;
+    lab.ensure(std::max<uint64_t>(n, 1) * 4);
+    if (n) launch_labels(c, m.parent, n, 1, lab.as<uint32_t>(), tiles.as<uint32_t>(), d_ncomp);
+    else CSB_CUDA(cudaMemsetAsync(d_ncomp, 0, 8, c.stream));
+    const uint64_t cap = n ? n - 1 : 0;
+    outb.ensure(std::max<uint64_t>(cap, 1) * sizeof(cs_edge));
+    launch_compact(c, m.bitmap, W, 1, tiles.as<uint32_t>() + nbl + 1, d_nedges, eu.as<uint32_t>(),
+                   ev.as<uint32_t>(), ew.as<float>(), nullptr, n, cap, outb.as<cs_edge>(), status);
+    check_launch(c, "MST finish");
+    status_check(c, status);
+    unsigned long long hcount[2];
+    uint64_t hbins[256];
+    CSB_CUDA(cudaMemcpyAsync(hcount, counts.p, 16, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaMemcpyAsync(hbins, bins.p, sizeof(hbins), cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    res->ncomp = static_cast<uint32_t>(hcount[0]);
+    res->nedges = hcount[1];
+    res->weight = exact_sum_from_bins(hbins);
+    if (out_edges && res->nedges) copy_d2h(c, out_edges, outb.p, res->nedges * sizeof(cs_edge));
+    if (out_labels && n) copy_d2h(c, out_labels, lab.p, static_cast<uint64_t>(n) * 4);
+}
+
+// ============================================================================
+// batched sweep
+// ============================================================================
+
+struct SweepPlan {
+    uint32_t n = 0, E = 0, K = 0, G = 0, W = 0, block = 0, grid = 0;
+    bool labels = false;
+    uint64_t edges_version = 0;
+    DevBuf mpts, core, parent, best, touched, wl, bitmap, bins, ctr, bar, status, tiles, lab, out, counts;
+    uint32_t nbl = 0, ntl = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool captured = false;
+    std::vector<uint32_t> host_mpts;
+    ~SweepPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+void sweep_free(SweepPlan* p) { delete p; }
+
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, std::pair<uint32_t, uint32_t>> g_tuned;
+
+SweepArgs args_of(Graph& g, SweepPlan& p) {
+    SweepArgs a;
+    a.n = p.n;
+    a.E = p.E;
+    a.K = p.K;
+    a.G = p.G;
+    a.W = p.W;
+    a.eu = g.eu.as<uint32_t>();
+    a.ev = g.ev.as<uint32_t>();
+    a.ew = g.ew.as<float>();
+    a.core = p.core.as<float>();
+    a.parent = p.parent.as<uint32_t>();
+    a.best = p.best.as<unsigned long long>();
+    a.touched = p.touched.as<uint32_t>();
+    a.wl = p.wl.as<uint32_t>();
+    a.bitmap = p.bitmap.as<uint32_t>();
+    a.bins = p.bins.as<unsigned long long>();
+    a.ctr = p.ctr.as<uint32_t>();
+    a.bar = p.bar.as<unsigned>();
+    a.status = p.status.as<int>();
+    a.limit_ns = kBarrierLimitNs;
+    return a;
+}
+
+/// Enqueue the whole sweep on the context stream (captured into the plan's graph).
+void enqueue_sweep(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    const uint64_t n = p.n;
+    CSB_CUDA(cudaMemsetAsync(p.status.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.bar.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.bitmap.p, 0, static_cast<uint64_t>(p.K) * p.W * 4, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.bins.p, 0, static_cast<uint64_t>(p.K) * 256 * 8, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.best.p, 0xFF, static_cast<uint64_t>(p.G) * std::max<uint64_t>(n, 1) * 8, c.stream));
+    if (n) {
+        k_core_multi<<<blocks_for(n), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(),
+                                                              p.n, g.k, p.mpts.as<uint32_t>(), p.K,
+                                                              p.core.as<float>());
+        count_launch(c);
+        SweepArgs a = args_of(g, p);
+        void* params[] = {&a};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(p.grid);
+        cfg.blockDim = dim3(p.block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = c.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
+        count_launch(c);
+        if (p.labels) {
+            launch_labels(c, p.parent.as<uint32_t>(), p.n, p.K, p.lab.as<uint32_t>(), p.tiles.as<uint32_t>(),
+                          p.counts.as<unsigned long long>());
+        }
+        launch_compact(c, p.bitmap.as<uint32_t>(), p.W, p.K,
+                       p.tiles.as<uint32_t>() + static_cast<uint64_t>(p.K) * p.nbl,
+                       p.counts.as<unsigned long long>() + p.K, g.eu.as<uint32_t>(), g.ev.as<uint32_t>(),
+                       g.ew.as<float>(), p.core.as<float>(), p.n, n ? n - 1 : 0, p.out.as<cs_edge>(),
+                       p.status.as<int>());
+    }
+}
+
+SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labels) {
+    Ctx& c = *g.ctx;
+    graph_build_edges(g);
+    SweepPlan* p = new SweepPlan();
+    try {
+        p->n = static_cast<uint32_t>(g.n);
+        p->E = static_cast<uint32_t>(g.e_total);
+        p->K = K;
+        p->G = std::max<uint32_t>(1, std::min<uint32_t>(G, std::min<uint32_t>(K, 32)));
+        p->W = (p->E + 31) / 32 + 1;
+        p->block = block;
+        p->labels = labels;
+        const uint64_t n = std::max<uint32_t>(p->n, 1);
+        const uint64_t E = std::max<uint32_t>(p->E, 1);
+        p->mpts.ensure(K * 4 + 4);
+        p->core.ensure(K * n * 4);
+        p->parent.ensure(K * n * 4);
+        p->best.ensure(p->G * n * 8);
+        p->touched.ensure(p->G * n * 4);
+        p->wl.ensure(p->G * 2 * E * 4);
+        p->bitmap.ensure(static_cast<uint64_t>(K) * p->W * 4);
+        p->bins.ensure(static_cast<uint64_t>(K) * 256 * 8);
+        p->ctr.ensure(static_cast<uint64_t>(p->G) * 8 * 4 + 64);
+        p->bar.ensure(64);
+        p->status.ensure(64);
+        p->nbl = blocks_for(n);
+        p->ntl = std::max<uint32_t>(1, (p->W + kTileWords - 1) / kTileWords);
+        p->tiles.ensure(static_cast<uint64_t>(K) * (p->nbl + p->ntl) * 4 + 64);
+        if (labels) p->lab.ensure(K * n * 4);
+        p->out.ensure(K * std::max<uint64_t>(n - 1, 1) * sizeof(cs_edge));
+        p->counts.ensure(static_cast<uint64_t>(2 * K) * 8 + 64);
+        int occ = 0;
+        CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep, static_cast<int>(block), 0));
+        if (occ < 1) fail(CS_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
+        p->grid = static_cast<uint32_t>(c.sm_count) * static_cast<uint32_t>(occ);
+        // capture the sweep into a CUDA graph
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CSB_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+        bool ok = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            const uint64_t before = c.launches;
+            try {
+                enqueue_sweep(g, *p);
+            } catch (...) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(c.stream, &junk);
+                if (junk) cudaGraphDestroy(junk);
+                cudaGetLastError();
+                ok = false;
+            }
+            c.launches = before;  // counted when replayed
+            if (ok) {
+                ok = cudaStreamEndCapture(c.stream, &p->graph) == cudaSuccess && p->graph;
+                if (ok) ok = cudaGraphInstantiate(&p->exec, p->graph, 0) == cudaSuccess;
+            }
+            if (!ok) cudaGetLastError();
+        }
+        p->captured = ok;
+    } catch (...) {
+        delete p;
+        throw;
+    }
+    return p;
+}
+
+uint64_t kernels_per_sweep(const SweepPlan& p) { return p.n ? (1 + 1 + (p.labels ? 4 : 0) + 3) : 0; }
+
+void run_plan(Graph& g, SweepPlan& p, float* out_ms) {
+    Ctx& c = *g.ctx;
+    cudaEvent_t e0, e1;
+    CSB_CUDA(cudaEventCreate(&e0));
+    CSB_CUDA(cudaEventCreate(&e1));
+    CSB_CUDA(cudaMemcpyAsync(p.mpts.p, p.host_mpts.data(), p.K * 4, cudaMemcpyHostToDevice, c.stream));
+    CSB_CUDA(cudaEventRecord(e0, c.stream));
+    if (p.captured) {
+        CSB_CUDA(cudaGraphLaunch(p.exec, c.stream));
+        count_launch(c, kernels_per_sweep(p));
+    } else {
+        enqueue_sweep(g, p);
+    }
+    CSB_CUDA(cudaEventRecord(e1, c.stream));
+    CSB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (out_ms) *out_ms = ms;
+    status_check(c, p.status.as<int>());
+}
+
+}  // namespace
+
+void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms) {
+    if (K == 0) fail(CS_ERR_INVALID, "sweep: K must be positive");
+    for (uint32_t j = 0; j < K; ++j) {
+        if (mpts[j] > g.k) fail(CS_ERR_INVALID, "sweep: mpts exceeds k_max");
+    }
+    graph_build_edges(g);
+    Ctx& c = *g.ctx;
+    uint32_t G = g.sweep_group, B = g.sweep_block;
+    if (!G || !B) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(std::make_tuple(static_cast<uint32_t>(g.n), static_cast<uint32_t>(g.e_total), K, c.sm_count));
+        if (it != g_tuned.end()) {
+            if (!G) G = it->second.first;
+            if (!B) B = it->second.second;
+        }
+    }
+    if (!G) G = std::min<uint32_t>(K, 4);
+    if (!B) B = 256;
+    SweepPlan* p = g.plan;
+    const bool reuse = p && p->n == g.n && p->E == g.e_total && p->K == K && p->G == std::min(G, std::min<uint32_t>(K, 32)) &&
+                       p->block == B && p->labels == want_labels && g.edges_valid;
+    if (!reuse) {
+        if (g.plan) sweep_free(g.plan);
+        g.plan = nullptr;
+        g.plan = make_plan(g, K, G, B, want_labels);
+        p = g.plan;
+    }
+    p->host_mpts.assign(mpts, mpts + K);
+    for (auto& m : p->host_mpts) {
+        if (m == 0) m = 1;  // CoreSG::edges treats mpts 0 as 1
+    }
+    run_plan(g, *p, out_ms);
+}
+
+void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res) {
+    SweepPlan* p = g.plan;
+    if (!p) fail(CS_ERR_STATE, "sweep_fetch: no sweep has run");
+    if (index >= p->K) fail(CS_ERR_INVALID, "sweep_fetch: index out of range");
+    if (out_labels && !p->labels) fail(CS_ERR_STATE, "sweep_fetch: the sweep ran without labels");
+    Ctx& c = *g.ctx;
+    unsigned long long ne = 0;
+    uint64_t bins[256];
+    CSB_CUDA(cudaMemcpyAsync(&ne, p->counts.as<unsigned long long>() + p->K + index, 8, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaMemcpyAsync(bins, p->bins.as<unsigned long long>() + static_cast<uint64_t>(index) * 256,
+                             sizeof(bins), cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    res->nedges = ne;
+    res->ncomp = static_cast<uint32_t>(p->n - ne);
+    res->weight = exact_sum_from_bins(bins);
+    const uint64_t cap = p->n ? p->n - 1 : 0;
+    if (out_edges && ne) copy_d2h(c, out_edges, p->out.as<cs_edge>() + index * cap, ne * sizeof(cs_edge));
+    if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(index) * p->n, static_cast<uint64_t>(p->n) * 4);
+}
+
+}  // namespace csb
+
+// ============================================================================
+// C API
+// ============================================================================
+
+using namespace csb;
+
+extern "C" {
+
+cs_status cs_extract(cs_graph* gp, uint32_t mpts, cs_edge* out_edges, uint32_t* out_labels,
+                     uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        MstHost r;
+        extract_plain(*g, mpts, out_edges, out_labels, &r);
+        if (out_nedges) *out_nedges = r.nedges;
+        if (out_ncomp) *out_ncomp = r.ncomp;
+        if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_extract_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
+                           uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
+                           double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep: null mpts");
+        sweep_run(*g, mpts, K, out_labels != nullptr, nullptr);
+        const uint64_t cap = g->n ? g->n - 1 : 0;
+        for (uint32_t j = 0; j < K; ++j) {
+            MstHost r;
+            sweep_fetch(*g, j, out_edges ? out_edges + j * cap : nullptr,
+                        out_labels ? out_labels + static_cast<uint64_t>(j) * g->n : nullptr, &r);
+            if (out_nedges) out_nedges[j] = r.nedges;
+            if (out_ncomp) out_ncomp[j] = r.ncomp;
+            if (out_weight) out_weight[j] = r.weight;
+        }
+    });
+}
+
+cs_status cs_extract_sweep_device(cs_graph* gp, const uint32_t* mpts, uint32_t K, float* out_ms) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep_device: null mpts");
+        sweep_run(*g, mpts, K, true, out_ms);
+    });
+}
+
+cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
+                         uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        MstHost r;
+        sweep_fetch(*g, index, out_edges, out_labels, &r);
+        if (out_nedges) *out_nedges = r.nedges;
+        if (out_ncomp) *out_ncomp = r.ncomp;
+        if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t group, uint32_t block_threads) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(block_threads == 0 || block_threads == 128 || block_threads == 256 || block_threads == 512,
+                    "cs_set_sweep_shape: block must be 128, 256 or 512");
+        CSB_REQUIRE(group <= 32, "cs_set_sweep_shape: group must be <= 32");
+        g->sweep_group = group;
+        g->sweep_block = block_threads;
+    });
+}
+
+cs_status cs_autotune_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, uint32_t* out_group,
+                            uint32_t* out_block) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr && K > 0, "cs_autotune_sweep: empty mpts");
+        const uint32_t saved_g = g->sweep_group, saved_b = g->sweep_block;
+        float best_ms = 1e30f;
+        uint32_t best_g = 0, best_b = 0;
+        const uint32_t groups[] = {1, 2, 4, 8, 16, 32};
+        const uint32_t blocks[] = {256, 512};
+        for (uint32_t G : groups) {
+            if (G > K && G != 1) continue;
+            for (uint32_t B : blocks) {
+                g->sweep_group = G;
+                g->sweep_block = B;
+                float ms = 0.0f, tot = 0.0f;
+                sweep_run(*g, mpts, K, true, &ms);  // build + warm
+                for (int rep = 0; rep < 2; ++rep) {
+                    sweep_run(*g, mpts, K, true, &ms);
+                    tot += ms;
+                }
+                if (tot < best_ms) {
+                    best_ms = tot;
+                    best_g = G;
+                    best_b = B;
+                }
+            }
+        }
+        g->sweep_group = saved_g;
+        g->sweep_block = saved_b;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tuned[std::make_tuple(static_cast<uint32_t>(g->n), static_cast<uint32_t>(g->e_total), K, g->ctx->sm_count)] =
+                std::make_pair(best_g, best_b);
+        }
+        if (out_group) *out_group = best_g;
+        if (out_block) *out_block = best_b;
+    });
+}
+
+}  // extern "C"
