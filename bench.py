@@ -1,0 +1,336 @@
+#!/usr/bin/env python3
+"""Benchmark of the CORE-SG hot path on B200.
+
+One step = one full mpts sweep (mpts = 1..k_max, K MSTs) over the device-resident
+CORE-SG of the workload, solved by the batched path: one persistent cooperative
+Boruvka launch replayed from a CUDA graph (cs_extract_sweep_device).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload blobs1m_d16]
+    python bench.py --impl reference ...   # the reference's own CPU path, same metric
+
+Reported (one JSON line from rank 0):
+  value      whole-job MSTs/s of the batched sweep, inputs resident in HBM, device
+             time (CUDA events on the engine stream), max over ranks
+  plain      the plain per-mpts GPU path (cs_extract: edges(mpts) materialised per call,
+             Boruvka rounds driven from the host) on the same graph
+  build_s    device CORE-SG build: NN-Descent + anti-hub bridges
+  e2e        the same metric through the C ABI with host buffers: the CORE-SG arrays
+             copied host->device and all K trees + labels copied back, every step
+  roofline   the persistent Boruvka kernel against the measured HBM copy bandwidth
+  cpu_baseline  the reference CPU extract (built from its sources) on the same
+             CORE-SG, a bounded sample of mpts values, all host threads
+Inputs: seeded synthetic Gaussian mixtures with the workload's shapes; the edge list
+(12 B x |E|, ~300 MB at n=1M) is larger than L2, so no L2 flush is needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "incremental-core-sg_b200"))
+
+METRIC = "mpts-sweep MSTs/s + build s, n=1M k=32 vs plain GPU path; p50/p99 query ms"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def sweep_bytes(n, E, K):
+    """Algorithmic bytes of one K-mpts sweep: the edge list once (u, v, w) plus,
+    per mpts, a core column and the output tree (12 B per tree edge)."""
+    return 12 * E + K * (4 * n + 12 * (n - 1))
+
+
+def sweep_kernel_bytes(n, E, K):
+    """Algorithmic bytes of the persistent kernel alone: the edge list once plus a
+    core column per mpts (its tree output is a bitmap, E/8 bytes per mpts)."""
+    return 12 * E + K * (4 * n + E // 8)
+
+
+# ---------------------------------------------------------------------------------------
+
+def run_reference(args):
+    """The reference's own CPU path (oracle/_ref: its sources compiled here) on the
+    same workload: CoreSG::build, then CoreSG::mst per mpts (the `coresg_cli extract`
+    loop); one step = one mpts value, all-in (edges(mpts) + MST)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from checkers import Reference
+    from coresg_b200.datagen import workload
+
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference built from source) is missing"}))
+        return 0
+    ref = Reference()
+    pts, w = workload(args.workload, args.n)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    sg = ref.build(pts, k_max=w["k_max"], instances=1, iters=10, sample=16, seed=42, threads=0)
+    build_s = time.perf_counter() - t0
+    log(f"[reference] build {build_s:.2f}s {sg.times}")
+    K = w["k_max"]
+    mp = [1 + (i % K) for i in range(args.warmup + args.steps)]
+    for m in mp[:args.warmup]:
+        sg.mst(m, algo=0)
+    secs = []
+    for m in mp[args.warmup:]:
+        r = sg.mst(m, algo=0)
+        secs.append(r["seconds_all"])
+    total = sum(secs)
+    value = len(secs) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n": w["n"], "dim": w["dim"], "k_max": w["k_max"],
+                   "step": "one CoreSG::mst(mpts) all-in, mpts cycling 1..k_max"},
+        "build_s": build_s,
+        "cpu_baseline": {"value": value, "unit": "MSTs/s", "cores": cores, "kind": "reference",
+                         "sample": f"{len(secs)} extractions (mpts {mp[args.warmup]}..), CoreSG::mst all-in"},
+        "e2e": {"value": value, "unit": "MSTs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges):
+    """The reference CPU extract on this CORE-SG (a bounded sample of mpts)."""
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from checkers import Reference
+        from coresg_b200.datagen import pad_rows
+
+        if not Reference.available():
+            return None
+        ref = Reference()
+        sg = ref.from_state(pad_rows(pts), w["dim"], ids, dists, flags, counts, bridges, threads=0)
+        sample = [1, 8, 16, w["k_max"]]
+        secs = [sg.mst(m, algo=0)["seconds_all"] for m in sample]
+        return {"value": len(sample) / sum(secs), "unit": "MSTs/s", "cores": os.cpu_count() or 1,
+                "kind": "reference",
+                "sample": f"CoreSG::mst all-in for mpts {sample} on this CORE-SG ({sum(secs):.1f} s)"}
+    except Exception as e:  # the baseline is reported, never required
+        log(f"[cpu_baseline] failed: {e}")
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="blobs1m_d16")
+    ap.add_argument("--n", type=int, default=None, help="override the workload's point count")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import coresg_b200 as cs
+    from coresg_b200.datagen import workload
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = cs.Context(local)
+    pts, w = workload(args.workload, args.n)
+    n, K = w["n"], w["k_max"]
+    mpts = list(range(1, K + 1))
+    g = cs.CoreSG(ctx, w["dim"], K)
+
+    # ---- build (device): NN-Descent + bridges
+    t0 = time.perf_counter()
+    st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42 + rank)
+    build_s = time.perf_counter() - t0
+    info = g.info()
+    E = info["knn_edges"] + info["bridges"]
+    log(f"[rank {rank}] build {build_s:.3f}s {st} |E|={E}")
+
+    # ---- batched sweep
+    group, block = g.autotune(mpts)
+    log(f"[rank {rank}] autotuned group={group} block={block}")
+    for _ in range(args.warmup):
+        g.sweep_device(mpts)
+    clk = Clocks(local)
+    barrier()
+    launches0 = ctx.launches
+    clk.start()
+    t_wall = time.perf_counter()
+    step_ms, kern_ms = [], []
+    for _ in range(args.steps):
+        step_ms.append(g.sweep_device(mpts))
+        kern_ms.append(g.sweep_timing()[1])
+    wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    launches = ctx.launches - launches0
+    barrier()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * K * args.steps / (total_ms / 1000.0)
+    ms_per_step = total_ms / args.steps
+    kernel_ms = float(np.mean(kern_ms))
+    log(f"[rank {rank}] sweep {ms_per_step:.3f} ms/step (kernel {kernel_ms:.3f} ms) wall {wall:.3f}s")
+
+    # ---- plain per-mpts path on the same graph (one pass over 1..K)
+    plain = None
+    if not args.no_plain:
+        ctx_l0 = ctx.launches
+        t1 = time.perf_counter()
+        for m in mpts:
+            cs.lib().cs_extract(g.h, m, None, None, None, None, None)
+        plain_s = time.perf_counter() - t1
+        plain = {"value": K / plain_s, "unit": "MSTs/s", "ms_per_mst": 1000 * plain_s / K,
+                 "kernel_launches": ctx.launches - ctx_l0,
+                 "what": "cs_extract per mpts: edges(mpts) materialised, Boruvka rounds host-driven"}
+
+    # ---- e2e through the C ABI with host buffers
+    ids, dists, flags, counts = g.knn()
+    bridges = g.missing_edges()
+    e2e = None
+    if args.e2e_steps > 0:
+        h2d = ids.nbytes + dists.nbytes + flags.nbytes + counts.nbytes + bridges.nbytes
+        secs, d2h = [], 0
+        for _ in range(args.e2e_steps):
+            t2 = time.perf_counter()
+            g.set_knn(ids, dists, flags, counts)
+            g.set_bridges(bridges)
+            res = g.all_msts(mpts, labels=True)
+            secs.append(time.perf_counter() - t2)
+            d2h = sum(r.edges.nbytes + r.component.nbytes + 20 for r in res)
+        e2e_s = max_over_ranks(sum(secs))
+        e2e = {"value": world * K * len(secs) / e2e_s, "unit": "MSTs/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": len(secs)}
+
+    # ---- roofline of the persistent kernel
+    peak, peak_kind = peaks()
+    kb = sweep_kernel_bytes(n, E, K)
+    achieved = kb / (kernel_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_sweep (persistent Boruvka, all K MSTs)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes": kb, "kernel_ms": kernel_ms,
+                "traffic": None,
+                "sweep_graph": {"algorithmic_bytes": sweep_bytes(n, E, K), "ms": ms_per_step,
+                                "achieved_gbs": sweep_bytes(n, E, K) / (ms_per_step / 1000.0) / 1e9}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "n": n, "dim": w["dim"], "k_max": K, "mpts": f"1..{K}",
+                       "edges": E, "knn_edges": info["knn_edges"], "bridges": info["bridges"],
+                       "sweep_group": group, "sweep_block": block,
+                       "l2": "inputs larger than L2 (edge list 12 B x |E|), no flush"},
+            "build_s": build_s, "build": st,
+            "plain": plain, "speedup_vs_plain": (value / world) / plain["value"] if plain else None,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks, "wall_s_timed": wall,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

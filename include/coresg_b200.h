@@ -198,6 +198,10 @@ cs_status cs_extract_sweep_device(cs_graph* g, const uint32_t* mpts, uint32_t K,
 cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
                          uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
 
+/* Device times of the last sweep: the whole captured sequence and the persistent
+ * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
+cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
+
 /* Sweep tuning knobs (group size = MSTs solved concurrently, block size); 0 picks
  * the cached autotuned value. */
 cs_status cs_set_sweep_shape(cs_graph* g, uint32_t group, uint32_t block_threads);

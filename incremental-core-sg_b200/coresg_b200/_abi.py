@@ -67,6 +67,7 @@ _SIGS = {
     "cs_extract_sweep": (_i32, [_p, _p, _u32, _p, _p, _p, _p, _p]),
     "cs_extract_sweep_device": (_i32, [_p, _p, _u32, _p]),
     "cs_sweep_fetch": (_i32, [_p, _u32, _p, _p, _p, _p, _p]),
+    "cs_sweep_timing": (_i32, [_p, _p, _p]),
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
 }
@@ -325,6 +326,12 @@ class CoreSG:
         self.ctx.check(lib().cs_sweep_fetch(self.h, index, _ptr(edges), _ptr(lab), C.byref(ne), C.byref(nc),
                                             C.byref(w)))
         return MstResult(edges[:ne.value], None if lab is None else lab[:n], nc.value, w.value)
+
+    def sweep_timing(self):
+        """(graph ms, persistent-kernel ms) of the last sweep."""
+        gm, km = C.c_float(), C.c_float()
+        self.ctx.check(lib().cs_sweep_timing(self.h, C.byref(gm), C.byref(km)))
+        return float(gm.value), float(km.value)
 
     def set_sweep_shape(self, group=0, block=0):
         self.ctx.check(lib().cs_set_sweep_shape(self.h, group, block))

@@ -1,24 +1,605 @@
-// Anti-hub bridges on the device (placeholder until the kernels land).
+// Anti-hub bridges on the device.
+//
+// Restates the bridge half of CoreSG::build/insert (src/coresg.cpp:472-516,
+// :537-583) with CoreSGParams/HubnessParams defaults:
+//
+//   connectivity  lock-free union-find over the k-NN adjacency, roots linked
+//                 larger-under-smaller, dense labels by first node
+//                 (ConnectivityTracker::rebuild, src/connectivity.cpp:24-139)
+//   hubness       reverse degrees by atomics, the arithmetic-mean reverse score in
+//                 double with the degenerate rules (src/hubness.cpp:44-158, :302-352)
+//   selection     the budget llround(d * ln|E|) capped by max_pair_ops (:16-40) lowest
+//                 under (score, rdeg, id) -- found by two 64-bit radix selects, one over
+//                 the score bits and one over (rdeg, id) among the score ties -- plus
+//                 the 2 lowest of every component (the reference's bucket scan keeps
+//                 exactly those, the order being strict); sorted by the same order
+//                 (:424-521)
+//   bridge MST    the m x m mutual-reachability matrix at k_max and Prim with the
+//                 lowest index winning ties, in one CTA; edges re-stored with their
+//                 base distance (mst_over_subset, src/coresg.cpp:97-141; mst_dense,
+//                 src/mst.cpp:268-330)
+//   repair        components left after the bridges are spanned through their
+//                 4 lowest-scoring members (repair_connectivity, src/coresg.cpp:171-258)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
 #include "common.cuh"
 #include "engine.hpp"
 
 namespace csb {
-void select_bridges(Graph& g, uint64_t*, uint64_t*, uint64_t*, uint32_t*) {
-    (void)g;
-    fail(CS_ERR_UNSUPPORTED, "cs_select_bridges: not built yet");
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kDenseLimit = 8192;  // CoreSGParams::dense_matrix_limit (coresg.hpp:88)
+
+inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
+    uint64_t b = (work + threads - 1) / threads;
+    return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(b, 1u << 30)));
 }
+
+__global__ void k_iota_u32(uint32_t* __restrict__ a, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+/// Unite every node with each of its listed neighbours.
+__global__ void k_conn_unite(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n,
+                             uint32_t k, uint32_t* __restrict__ parent, int* status) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<uint64_t>(n) * k) return;
+    const uint32_t p = static_cast<uint32_t>(t / k), j = static_cast<uint32_t>(t % k);
+    if (j >= counts[p]) return;
+    const uint32_t q = ids[t];
+    if (q < n && q != p) uf_unite(parent, p, q, status);
+}
+
+__global__ void k_rdeg(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
+                       int* __restrict__ rdeg) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<uint64_t>(n) * k) return;
+    const uint32_t p = static_cast<uint32_t>(t / k), j = static_cast<uint32_t>(t % k);
+    if (j >= counts[p]) return;
+    const uint32_t q = ids[t];
+    if (q < n) atomicAdd(rdeg + q, 1);
+}
+
+/// compute_score, arithmetic mean (src/hubness.cpp:302-352); IEEE double division.
+__global__ void k_score(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
+                        uint32_t k_for_score, const int* __restrict__ rdeg, double* __restrict__ score,
+                        unsigned long long* __restrict__ key_score, unsigned long long* __restrict__ key_tie) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const uint32_t deg = counts[v];
+    const int rd = rdeg[v];
+    long long sum = 0;
+    for (uint32_t j = 0; j < deg; ++j) {
+        const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
+        if (q < n) sum += rdeg[q];
+    }
+    double s;
+    if (rd > 0 && sum <= 0) s = static_cast<double>(k_for_score);
+    else if (rd <= 0 && sum > 0) s = 0.0;
+    else if (rd <= 0 && sum <= 0) s = 1.0;
+    else if (deg == 0) s = 1.0;
+    else {
+        const double denom = __ddiv_rn(static_cast<double>(sum), static_cast<double>(deg));
+        s = denom > 0.0 ? __ddiv_rn(static_cast<double>(rd), denom) : static_cast<double>(k_for_score);
+    }
+    score[v] = s;
+    // scores are >= 0, so their bit patterns order like the values
+    key_score[v] = static_cast<unsigned long long>(__double_as_longlong(s));
+    key_tie[v] = (static_cast<unsigned long long>(static_cast<uint32_t>(rd)) << 32) | v;
+}
+
+/// Histogram of one 8-bit digit of key[] over the elements whose higher digits
+/// equal `prefix` (and, when tie_key != null, whose tie_key equals tie_value).
+__global__ void k_digit_hist(const unsigned long long* __restrict__ key, uint32_t n, int shift,
+                             unsigned long long prefix, unsigned long long pmask,
+                             const unsigned long long* __restrict__ filt, unsigned long long filt_value,
+                             uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < n; v += stride) {
+        if (filt && filt[v] != filt_value) continue;
+        const unsigned long long x = key[v];
+        if ((x & pmask) != prefix) continue;
+        atomicAdd(h + ((x >> shift) & 0xFFu), 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        if (h[i]) atomicAdd(hist + i, h[i]);
+    }
+}
+
+/// Collect v with score < T, or score == T and tie <= T2 (selection of the budget).
+__global__ void k_collect(const unsigned long long* __restrict__ ks, const unsigned long long* __restrict__ kt,
+                          uint32_t n, unsigned long long T, unsigned long long T2, int use_ties,
+                          uint8_t* __restrict__ chosen, uint32_t* __restrict__ out, uint32_t* __restrict__ cnt,
+                          uint32_t cap) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const bool take = ks[v] < T || (use_ties && ks[v] == T && kt[v] <= T2);
+    if (!take) return;
+    chosen[v] = 1;
+    const uint32_t pos = atomicAdd(cnt, 1u);
+    if (pos < cap) out[pos] = v;
+}
+
+/// One quota round: per component, the lowest (score) then lowest (rdeg, id) among
+/// the nodes not yet taken by an earlier quota round.
+__global__ void k_quota_score(const unsigned long long* __restrict__ ks, const uint32_t* __restrict__ comp, uint32_t n,
+                              const uint8_t* __restrict__ qtaken, unsigned long long* __restrict__ best_s) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || qtaken[v]) return;
+    atomicMin(best_s + comp[v], ks[v]);
+}
+__global__ void k_quota_tie(const unsigned long long* __restrict__ ks, const unsigned long long* __restrict__ kt,
+                            const uint32_t* __restrict__ comp, uint32_t n, const uint8_t* __restrict__ qtaken,
+                            const unsigned long long* __restrict__ best_s, unsigned long long* __restrict__ best_t) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || qtaken[v]) return;
+    const uint32_t c = comp[v];
+    if (ks[v] == best_s[c]) atomicMin(best_t + c, kt[v]);
+}
+__global__ void k_quota_take(const unsigned long long* __restrict__ best_t, uint32_t ncomp,
+                             uint8_t* __restrict__ qtaken, uint8_t* __restrict__ chosen, uint32_t* __restrict__ out,
+                             uint32_t* __restrict__ cnt, uint32_t cap) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncomp) return;
+    const unsigned long long t = best_t[c];
+    if (t == kNoKey) return;
+    const uint32_t v = static_cast<uint32_t>(t);
+    qtaken[v] = 1;
+    if (!chosen[v]) {
+        chosen[v] = 1;
+        const uint32_t pos = atomicAdd(cnt, 1u);
+        if (pos < cap) out[pos] = v;
+    }
+}
+
+/// Gather the selected rows and their k_max core distances.
+__global__ void k_gather(const float* __restrict__ pts, uint32_t stride, const float* __restrict__ dists,
+                         const uint32_t* __restrict__ counts, uint32_t k, const uint32_t* __restrict__ sel, uint32_t m,
+                         float* __restrict__ out_pts, float* __restrict__ out_core) {
+    const uint32_t i = blockIdx.x;
+    if (i >= m) return;
+    const uint32_t v = sel[i];
+    for (uint32_t d = threadIdx.x; d < stride; d += blockDim.x) out_pts[static_cast<uint64_t>(i) * stride + d] = pts[static_cast<uint64_t>(v) * stride + d];
+    if (threadIdx.x == 0) out_core[i] = core_of(dists, counts, k, v, k);
+}
+
+/// Rows [r0, r1) of the m x m mutual-reachability matrix (mrd_block_kernel,
+/// cuda/mrd_kernels.cu:30-87, with the CPU backend's association order so the
+/// values equal src/cpu_backend.cpp:61-90 bit for bit).
+__global__ void k_mrd(const float* __restrict__ pts, uint32_t m, uint32_t stride, int metric,
+                      const float* __restrict__ core, uint32_t r0, uint32_t rows, float* __restrict__ out) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<uint64_t>(rows) * m) return;
+    const uint32_t lr = static_cast<uint32_t>(t / m), j = static_cast<uint32_t>(t % m);
+    const uint32_t i = r0 + lr;
+    float v;
+    if (i == j) {
+        v = 0.0f;
+    } else {
+        const float d = finalize_rank(l2sqr_ref(pts + static_cast<uint64_t>(i) * stride, pts + static_cast<uint64_t>(j) * stride, stride), metric);
+        v = max_ref(d, max_ref(core[i], core[j]));
+    }
+    out[t] = v;
+}
+
+/// Prim over the dense matrix in one CTA (mst_prim_virtual, src/mst.cpp:274-330):
+/// start at 0, relax from the current row, pick the smallest best[] with the lowest
+/// index winning ties; edges carry the base distance of their endpoints
+/// (src/coresg.cpp:346-351) and global ids via `ids`.
+__global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* __restrict__ pts, uint32_t stride,
+                       int metric, const uint32_t* __restrict__ ids, float* __restrict__ best, uint32_t* __restrict__ from,
+                       uint8_t* __restrict__ in_tree, cs_edge* __restrict__ out, uint32_t* __restrict__ out_count) {
+    __shared__ unsigned long long red[1024 / 32];
+    __shared__ uint32_t s_pick;
+    __shared__ float s_pick_w;
+    __shared__ uint32_t s_cnt;
+    const float inf = __int_as_float(0x7f800000);
+    for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+        best[j] = inf;
+        from[j] = kInvalid;
+        in_tree[j] = 0;
+    }
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        in_tree[0] = 1;
+        best[0] = 0.0f;
+    }
+    __syncthreads();
+    uint32_t current = 0;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t step = 1; step < m; ++step) {
+        const float* row = mat + static_cast<uint64_t>(current) * m;
+        // relax, then argmin over (best bits, index): ties -> lowest index, and an
+        // all-infinite frontier still picks its lowest index (the reference's rule)
+        unsigned long long mine = kNoKey;
+        for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+            if (in_tree[j]) continue;
+            const float w = row[j];
+            if (w < best[j]) {
+                best[j] = w;
+                from[j] = current;
+            }
+            const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(best[j])) << 32) | j;
+            mine = key < mine ? key : mine;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xFFFFFFFFu, mine, o);
+            mine = other < mine ? other : mine;
+        }
+        if (lane == 0) red[warp] = mine;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long b = kNoKey;
+            for (unsigned w2 = 0; w2 < nw; ++w2) b = red[w2] < b ? red[w2] : b;
+            s_pick = b == kNoKey ? kInvalid : static_cast<uint32_t>(b);
+            s_pick_w = b == kNoKey ? inf : __uint_as_float(static_cast<uint32_t>(b >> 32));
+            if (s_pick != kInvalid) {
+                in_tree[s_pick] = 1;
+                if (from[s_pick] != kInvalid && s_pick_w < inf) {
+                    const uint32_t a = from[s_pick], bb = s_pick;
+                    const float base = finalize_rank(l2sqr_ref(pts + static_cast<uint64_t>(a) * stride, pts + static_cast<uint64_t>(bb) * stride, stride), metric);
+                    const uint32_t ga = ids[a], gb = ids[bb];
+                    cs_edge e;
+                    e.u = ga < gb ? ga : gb;
+                    e.v = ga < gb ? gb : ga;
+                    e.w = base;
+                    out[s_cnt++] = e;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_pick == kInvalid) break;
+        current = s_pick;
+    }
+    if (threadIdx.x == 0) *out_count = s_cnt;
+}
+
+struct Scratch {
+    DevBuf parent, lab, bc, ncomp, rdeg, score, ks, kt, hist, chosen, qtaken, sel, selcnt, best_s, best_t,
+        sub_pts, sub_core, mat, pbest, pfrom, pintree, pout, pcnt;
+};
+
+/// Smallest threshold T over key[] (restricted by the filter) with
+/// count(key <= T) >= rank (1-based), by 8-bit radix passes from the top.
+unsigned long long radix_select(Ctx& c, Scratch& s, const unsigned long long* key, uint32_t n, uint64_t rank,
+                                const unsigned long long* filt, unsigned long long filt_value) {
+    unsigned long long prefix = 0, pmask = 0;
+    uint64_t remaining = rank;
+    uint32_t h[256];
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        CSB_CUDA(cudaMemsetAsync(s.hist.p, 0, 256 * 4, c.stream));
+        k_digit_hist<<<std::min<unsigned>(blocks_for(n), 4u * c.sm_count), kThreads, 0, c.stream>>>(
+            key, n, shift, prefix, pmask, filt, filt_value, s.hist.as<uint32_t>());
+        count_launch(c);
+        CSB_CUDA(cudaMemcpyAsync(h, s.hist.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        uint32_t d = 0;
+        uint64_t acc = 0;
+        for (; d < 256; ++d) {
+            if (acc + h[d] >= remaining) break;
+            acc += h[d];
+        }
+        if (d == 256) fail(CS_ERR_STATE, "radix select: rank beyond the population");
+        remaining -= acc;
+        prefix |= static_cast<unsigned long long>(d) << shift;
+        pmask |= 0xFFull << shift;
+    }
+    return prefix;
+}
+
+/// Dense MRD matrix + Prim over `m` selected nodes (device ids in d_sel); appends
+/// the edges (global ids, base distances) to `out`.
+void mst_over_subset(Graph& g, Scratch& s, const uint32_t* d_sel, uint32_t m, std::vector<cs_edge>* out) {
+    Ctx& c = *g.ctx;
+    if (m < 2) return;
+    if (m > kDenseLimit) fail(CS_ERR_UNSUPPORTED, "bridge MST over more than 8192 nodes (streamed Prim) is not built");
+    s.sub_pts.ensure(static_cast<uint64_t>(m) * g.stride * 4);
+    s.sub_core.ensure(m * 4ull);
+    s.mat.ensure(static_cast<uint64_t>(m) * m * 4);
+    s.pbest.ensure(m * 4ull);
+    s.pfrom.ensure(m * 4ull);
+    s.pintree.ensure(m + 16ull);
+    s.pout.ensure(m * sizeof(cs_edge) + 64);
+    s.pcnt.ensure(64);
+    k_gather<<<m, 128, 0, c.stream>>>(g.pts.as<float>(), g.stride, g.dists.as<float>(), g.counts.as<uint32_t>(), g.k, d_sel,
+                                       m, s.sub_pts.as<float>(), s.sub_core.as<float>());
+    const uint64_t cells = static_cast<uint64_t>(m) * m;
+    k_mrd<<<blocks_for(cells), kThreads, 0, c.stream>>>(s.sub_pts.as<float>(), m, g.stride, g.metric, s.sub_core.as<float>(),
+                                                       0, m, s.mat.as<float>());
+    k_prim<<<1, 1024, 0, c.stream>>>(s.mat.as<float>(), m, s.sub_pts.as<float>(), g.stride, g.metric, d_sel,
+                                     s.pbest.as<float>(), s.pfrom.as<uint32_t>(), s.pintree.as<uint8_t>(),
+                                     s.pout.as<cs_edge>(), s.pcnt.as<uint32_t>());
+    count_launch(c, 3);
+    check_launch(c, "bridge MST");
+    uint32_t cnt = 0;
+    CSB_CUDA(cudaMemcpyAsync(&cnt, s.pcnt.p, 4, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<cs_edge> e(cnt);
+    if (cnt) copy_d2h(c, e.data(), s.pout.p, cnt * sizeof(cs_edge));
+    out->insert(out->end(), e.begin(), e.end());
+}
+
+// host-side union-find over component labels (a few thousand at most)
+struct HostUF {
+    std::vector<uint32_t> p;
+    explicit HostUF(uint32_t n) : p(n) { std::iota(p.begin(), p.end(), 0u); }
+    uint32_t find(uint32_t x) {
+        while (p[x] != x) x = p[x] = p[p[x]];
+        return x;
+    }
+    bool unite(uint32_t a, uint32_t b) {
+        a = find(a);
+        b = find(b);
+        if (a == b) return false;
+        if (a > b) std::swap(a, b);
+        p[b] = a;
+        return true;
+    }
+};
+
+}  // namespace
+
+void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metric, const float* d_core, uint32_t r0,
+              uint32_t r1, float* d_out) {
+    const uint64_t cells = static_cast<uint64_t>(r1 - r0) * m;
+    if (!cells) return;
+    k_mrd<<<blocks_for(cells), kThreads, 0, c.stream>>>(d_pts, m, stride, metric, d_core, r0, r1 - r0, d_out);
+    count_launch(c);
+    check_launch(c, "mrd rows");
+}
+
+void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
+                    uint32_t* out_components) {
+    Ctx& c = *g.ctx;
+    const uint32_t n = static_cast<uint32_t>(g.n);
+    const uint32_t k = g.k;
+    CSB_REQUIRE(n > 0, "cs_select_bridges: empty graph");
+    Scratch s;
+    int* status = c.status.as<int>();
+    CSB_CUDA(cudaMemsetAsync(status, 0, 4, c.stream));
+    const uint64_t nk = static_cast<uint64_t>(n) * k;
+    // ---- connectivity
+    s.parent.ensure(n * 4ull);
+    s.lab.ensure(n * 4ull);
+    const uint32_t nb = blocks_for(n);
+    s.bc.ensure(nb * 4ull + 64);
+    s.ncomp.ensure(64);
+    k_iota_u32<<<blocks_for(n), kThreads, 0, c.stream>>>(s.parent.as<uint32_t>(), n);
+    k_conn_unite<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k,
+                                                            s.parent.as<uint32_t>(), status);
+    count_launch(c, 2);
+    launch_labels(c, s.parent.as<uint32_t>(), n, 1, s.lab.as<uint32_t>(), s.bc.as<uint32_t>(),
+                  s.ncomp.as<unsigned long long>());
+    // ---- hubness
+    s.rdeg.ensure(n * 4ull);
+    s.score.ensure(n * 8ull);
+    s.ks.ensure(n * 8ull);
+    s.kt.ensure(n * 8ull);
+    CSB_CUDA(cudaMemsetAsync(s.rdeg.p, 0, n * 4ull, c.stream));
+    k_rdeg<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, s.rdeg.as<int>());
+    k_score<<<blocks_for(n), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, k,
+                                                      s.rdeg.as<int>(), s.score.as<double>(),
+                                                      s.ks.as<unsigned long long>(), s.kt.as<unsigned long long>());
+    count_launch(c, 2);
+    check_launch(c, "hubness");
+    unsigned long long ncomp64 = 0;
+    CSB_CUDA(cudaMemcpyAsync(&ncomp64, s.ncomp.p, 8, cudaMemcpyDeviceToHost, c.stream));
+    int st = 0;
+    CSB_CUDA(cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "connectivity: a union retry loop ran out");
+    const uint32_t ncomp = static_cast<uint32_t>(ncomp64);
+    // ---- budget (host arithmetic identical to antihub_budget)
+    graph_build_edges(g);
+    const uint64_t num_edges = g.e_knn;
+    const double logs = num_edges > 1 ? std::log(static_cast<double>(num_edges)) : 0.0;
+    double raw = 1.0 * static_cast<double>(g.dim) * logs;
+    if (!(raw > 0.0)) raw = 0.0;
+    uint64_t budget = static_cast<uint64_t>(std::llround(raw));
+    {
+        const double m_max = std::sqrt(2.0 * 2e9 / static_cast<double>(g.dim));
+        if (m_max >= 1.0 && static_cast<double>(budget) > m_max) budget = static_cast<uint64_t>(m_max);
+    }
+    if (budget < 2) budget = 2;
+    if (budget > n) budget = n;
+    // ---- selection: budget lowest under (score, rdeg, id)
+    const uint32_t cap = static_cast<uint32_t>(budget + 2ull * ncomp + 8);
+    s.hist.ensure(256 * 4);
+    s.chosen.ensure(n + 16ull);
+    s.qtaken.ensure(n + 16ull);
+    s.sel.ensure(cap * 4ull);
+    s.selcnt.ensure(64);
+    CSB_CUDA(cudaMemsetAsync(s.chosen.p, 0, n, c.stream));
+    CSB_CUDA(cudaMemsetAsync(s.qtaken.p, 0, n, c.stream));
+    CSB_CUDA(cudaMemsetAsync(s.selcnt.p, 0, 64, c.stream));
+    const unsigned long long* ks = s.ks.as<unsigned long long>();
+    const unsigned long long* kt = s.kt.as<unsigned long long>();
+    if (budget > 0) {
+        const unsigned long long T = radix_select(c, s, ks, n, budget, nullptr, 0);
+        // count strictly below T
+        unsigned long long T2 = 0;
+        int use_ties = 0;
+        {
+            // population of score < T = budget - (rank of the needed ties)
+            uint64_t below = 0;
+            // histogram-free count: reuse radix select on ks with rank = budget gives T;
+            // the ties needed = budget - count(ks < T); count it with one more pass
+            DevBuf tmpc;
+            tmpc.ensure(64);
+            CSB_CUDA(cudaMemsetAsync(tmpc.p, 0, 64, c.stream));
+            k_collect<<<blocks_for(n), kThreads, 0, c.stream>>>(ks, kt, n, T, 0, 0, s.chosen.as<uint8_t>(),
+                                                                 s.sel.as<uint32_t>(), tmpc.as<uint32_t>(), cap);
+            count_launch(c);
+            uint32_t hb = 0;
+            CSB_CUDA(cudaMemcpyAsync(&hb, tmpc.p, 4, cudaMemcpyDeviceToHost, c.stream));
+            CSB_CUDA(cudaStreamSynchronize(c.stream));
+            below = hb;
+            if (below < budget) {
+                T2 = radix_select(c, s, kt, n, budget - below, ks, T);
+                use_ties = 1;
+            }
+            // redo the collection with the tie rule into the real list
+            CSB_CUDA(cudaMemsetAsync(s.chosen.p, 0, n, c.stream));
+            k_collect<<<blocks_for(n), kThreads, 0, c.stream>>>(ks, kt, n, T, T2, use_ties, s.chosen.as<uint8_t>(),
+                                                                 s.sel.as<uint32_t>(), s.selcnt.as<uint32_t>(), cap);
+            count_launch(c);
+        }
+    }
+    // ---- per-component quota (2 lowest of every component)
+    s.best_s.ensure(std::max<uint32_t>(ncomp, 1) * 8ull);
+    s.best_t.ensure(std::max<uint32_t>(ncomp, 1) * 8ull);
+    for (int round = 0; round < 2 && ncomp > 0; ++round) {
+        CSB_CUDA(cudaMemsetAsync(s.best_s.p, 0xFF, ncomp * 8ull, c.stream));
+        CSB_CUDA(cudaMemsetAsync(s.best_t.p, 0xFF, ncomp * 8ull, c.stream));
+        k_quota_score<<<blocks_for(n), kThreads, 0, c.stream>>>(ks, s.lab.as<uint32_t>(), n, s.qtaken.as<uint8_t>(),
+                                                                s.best_s.as<unsigned long long>());
+        k_quota_tie<<<blocks_for(n), kThreads, 0, c.stream>>>(ks, kt, s.lab.as<uint32_t>(), n, s.qtaken.as<uint8_t>(),
+                                                              s.best_s.as<unsigned long long>(),
+                                                              s.best_t.as<unsigned long long>());
+        k_quota_take<<<blocks_for(ncomp), kThreads, 0, c.stream>>>(s.best_t.as<unsigned long long>(), ncomp,
+                                                                   s.qtaken.as<uint8_t>(), s.chosen.as<uint8_t>(),
+                                                                   s.sel.as<uint32_t>(), s.selcnt.as<uint32_t>(), cap);
+        count_launch(c, 3);
+    }
+    check_launch(c, "selection");
+    uint32_t m = 0;
+    CSB_CUDA(cudaMemcpyAsync(&m, s.selcnt.p, 4, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    if (m > cap) fail(CS_ERR_STATE, "selection overflow");
+    // order the (few hundred) selected ids by (score, rdeg, id) on the host
+    std::vector<uint32_t> sel(m);
+    std::vector<unsigned long long> hks(n), hkt;
+    copy_d2h(c, sel.data(), s.sel.p, m * 4ull);
+    {
+        std::vector<unsigned long long> sk(m), tk(m);
+        // gather the keys of the selected ids
+        std::vector<unsigned long long> all_ks(n), all_kt(n);
+        copy_d2h(c, all_ks.data(), s.ks.p, n * 8ull);
+        copy_d2h(c, all_kt.data(), s.kt.p, n * 8ull);
+        std::sort(sel.begin(), sel.end(), [&](uint32_t a, uint32_t b) {
+            if (all_ks[a] != all_ks[b]) return all_ks[a] < all_ks[b];
+            return all_kt[a] < all_kt[b];
+        });
+        hks.swap(all_ks);
+        hkt.swap(all_kt);
+    }
+    g.selected = sel;
+    copy_h2d(c, s.sel.p, sel.data(), m * 4ull);
+    // ---- bridge MST over the selected set
+    std::vector<cs_edge> missing;
+    mst_over_subset(g, s, s.sel.as<uint32_t>(), m, &missing);
+    // ---- repair_connectivity
+    uint64_t added = 0;
+    {
+        std::vector<uint32_t> lab(n);
+        copy_d2h(c, lab.data(), s.lab.p, n * 4ull);
+        HostUF uf(ncomp);
+        for (const cs_edge& e : missing) uf.unite(lab[e.u], lab[e.v]);
+        // merged dense labels, numbered by first component (UnionFind::labels)
+        std::vector<uint32_t> merged(ncomp), remap(ncomp, kInvalid);
+        uint32_t nc2 = 0;
+        for (uint32_t cc = 0; cc < ncomp; ++cc) {
+            const uint32_t r = uf.find(cc);
+            if (remap[r] == kInvalid) remap[r] = nc2++;
+            merged[cc] = remap[r];
+        }
+        if (nc2 > 1) {
+            std::vector<double> score(n);
+            copy_d2h(c, score.data(), s.score.p, n * 8ull);
+            uint64_t per = 4;
+            if (static_cast<uint64_t>(nc2) * per > 4096) per = std::max<uint64_t>(1, 4096 / nc2);
+            std::vector<std::vector<uint32_t>> buckets(nc2);
+            for (uint32_t v = 0; v < n; ++v) {
+                std::vector<uint32_t>& b = buckets[merged[lab[v]]];
+                if (b.size() < per) {
+                    b.push_back(v);
+                } else {
+                    size_t worst = 0;
+                    for (size_t t = 1; t < b.size(); ++t) {
+                        if (score[b[t]] > score[b[worst]]) worst = t;
+                    }
+                    if (score[v] < score[b[worst]]) b[worst] = v;
+                }
+            }
+            std::vector<uint32_t> reps;
+            for (const auto& b : buckets) reps.insert(reps.end(), b.begin(), b.end());
+            if (reps.size() > 4096) {
+                std::partial_sort(reps.begin(), reps.begin() + 4096, reps.end(),
+                                  [&](uint32_t a, uint32_t b) { return score[a] < score[b]; });
+                reps.resize(4096);
+            }
+            if (reps.size() >= 2) {
+                DevBuf d_reps;
+                d_reps.ensure(reps.size() * 4);
+                copy_h2d(c, d_reps.p, reps.data(), reps.size() * 4);
+                std::vector<cs_edge> rep_mst;
+                mst_over_subset(g, s, d_reps.as<uint32_t>(), static_cast<uint32_t>(reps.size()), &rep_mst);
+                HostUF cuf(nc2);
+                for (const cs_edge& e : rep_mst) {
+                    if (cuf.unite(merged[lab[e.u]], merged[lab[e.v]])) {
+                        missing.push_back(e);
+                        ++added;
+                    }
+                }
+            }
+        }
+    }
+    // ---- install the bridges
+    g.bridges.ensure(std::max<size_t>(missing.size(), 1) * sizeof(cs_edge));
+    if (!missing.empty()) copy_h2d(c, g.bridges.p, missing.data(), missing.size() * sizeof(cs_edge));
+    g.nb = missing.size();
+    g.n_repair = added;
+    g.invalidate_edges();
+    if (out_selected) *out_selected = m;
+    if (out_bridges) *out_bridges = missing.size();
+    if (out_repair) *out_repair = added;
+    if (out_components) *out_components = ncomp;
+}
+
 }  // namespace csb
 
 using namespace csb;
+
 extern "C" {
-cs_status cs_mrd_block(cs_ctx* ctx, const float*, size_t, uint32_t, uint32_t, int32_t, const float*, size_t,
-                       size_t, float*) {
-    return guarded(reinterpret_cast<Ctx*>(ctx), [&] { fail(CS_ERR_UNSUPPORTED, "cs_mrd_block: not built yet"); });
+
+cs_status cs_mrd_block(cs_ctx* ctx, const float* host_pts, size_t m, uint32_t dim, uint32_t stride, int32_t metric,
+                       const float* host_core, size_t r0, size_t r1, float* host_out) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    return guarded(c, [&] {
+        (void)dim;
+        if (m == 0 || r1 <= r0) return;
+        CSB_REQUIRE(host_pts && host_core && host_out, "cs_mrd_block: null buffer");
+        CSB_REQUIRE(r1 <= m && stride % 8 == 0 && stride >= dim, "cs_mrd_block: bad range or stride");
+        if (metric != CS_METRIC_L2 && metric != CS_METRIC_COSINE)
+            fail(CS_ERR_UNSUPPORTED, "mrd_block_gpu: unsupported metric for the device path");
+        DevBuf pts, core, out;
+        pts.ensure(m * stride * 4);
+        core.ensure(m * 4);
+        out.ensure((r1 - r0) * m * 4);
+        copy_h2d(*c, pts.p, host_pts, m * stride * 4);
+        copy_h2d(*c, core.p, host_core, m * 4);
+        mrd_rows(*c, pts.as<float>(), static_cast<uint32_t>(m), stride, metric, core.as<float>(),
+                 static_cast<uint32_t>(r0), static_cast<uint32_t>(r1), out.as<float>());
+        copy_d2h(*c, host_out, out.p, (r1 - r0) * m * 4);
+    });
 }
-cs_status cs_select_bridges(cs_graph* gp, uint64_t* a, uint64_t* b, uint64_t* c, uint32_t* d) {
+
+cs_status cs_select_bridges(cs_graph* gp, uint64_t* a, uint64_t* b, uint64_t* cc, uint32_t* d) {
     Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] { select_bridges(*g, a, b, c, d); });
+    return guarded(g ? g->ctx : nullptr, [&] { select_bridges(*g, a, b, cc, d); });
 }
+
 cs_status cs_get_selected(cs_graph* gp, uint32_t* out, uint64_t cap, uint64_t* out_count) {
     Graph* g = reinterpret_cast<Graph*>(gp);
     return guarded(g ? g->ctx : nullptr, [&] {
@@ -26,4 +607,5 @@ cs_status cs_get_selected(cs_graph* gp, uint32_t* out, uint64_t cap, uint64_t* o
         for (uint64_t i = 0; out && i < cap && i < g->selected.size(); ++i) out[i] = g->selected[i];
     });
 }
-}
+
+}  // extern "C"

@@ -142,6 +142,10 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
 void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
 void sweep_free(SweepPlan* p);
 double exact_sum_from_bins(const uint64_t* bins256);
+/// Dense labels (numbered by smallest node) of K union-find forests parent_all[K][n]
+/// whose roots are their sets' smallest nodes; component counts -> ncomp[K].
+void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_t* lab_all, uint32_t* bc,
+                   unsigned long long* ncomp);
 
 // knn.cu
 void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,

@@ -519,8 +519,6 @@ double exact_sum_from_bins(const uint64_t* bins) {
 // shared finishing: labels + compaction for K MSTs
 // ============================================================================
 
-namespace {
-
 void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_t* lab_all,
                    uint32_t* bc, unsigned long long* ncomp) {
     const uint32_t nb = blocks_for(n);
@@ -531,6 +529,8 @@ void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_
     k_label_fill<<<grid, kThreads, 0, c.stream>>>(parent_all, n, lab_all);
     count_launch(c, 4);
 }
+
+namespace {
 
 void launch_compact(Ctx& c, const uint32_t* bitmap, uint32_t W, uint32_t K, uint32_t* tiles,
                     unsigned long long* nedges, const uint32_t* eu, const uint32_t* ev, const float* ew,
@@ -665,9 +665,14 @@ struct SweepPlan {
     cudaGraphExec_t exec = nullptr;
     bool captured = false;
     std::vector<uint32_t> host_mpts;
+    const void* key_ptrs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;  // around the persistent kernel
+    float last_graph_ms = 0.0f, last_kernel_ms = 0.0f;
     ~SweepPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (ev_k0) cudaEventDestroy(ev_k0);
+        if (ev_k1) cudaEventDestroy(ev_k1);
     }
 };
 
@@ -728,7 +733,9 @@ void enqueue_sweep(Graph& g, SweepPlan& p) {
         attr[0].val.cooperative = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        CSB_CUDA(cudaEventRecord(p.ev_k0, c.stream));
         CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
+        CSB_CUDA(cudaEventRecord(p.ev_k1, c.stream));
         count_launch(c);
         if (p.labels) {
             launch_labels(c, p.parent.as<uint32_t>(), p.n, p.K, p.lab.as<uint32_t>(), p.tiles.as<uint32_t>(),
@@ -749,6 +756,13 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labe
     try {
         p->n = static_cast<uint32_t>(g.n);
         p->E = static_cast<uint32_t>(g.e_total);
+        p->key_ptrs[0] = g.eu.p;
+        p->key_ptrs[1] = g.ev.p;
+        p->key_ptrs[2] = g.ew.p;
+        p->key_ptrs[3] = g.dists.p;
+        p->key_ptrs[4] = g.counts.p;
+        CSB_CUDA(cudaEventCreate(&p->ev_k0));
+        CSB_CUDA(cudaEventCreate(&p->ev_k1));
         p->K = K;
         p->G = std::max<uint32_t>(1, std::min<uint32_t>(G, std::min<uint32_t>(K, 32)));
         p->W = (p->E + 31) / 32 + 1;
@@ -824,10 +838,13 @@ void run_plan(Graph& g, SweepPlan& p, float* out_ms) {
     }
     CSB_CUDA(cudaEventRecord(e1, c.stream));
     CSB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.0f;
+    float ms = 0.0f, kms = 0.0f;
     CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (p.n) CSB_CUDA(cudaEventElapsedTime(&kms, p.ev_k0, p.ev_k1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    p.last_graph_ms = ms;
+    p.last_kernel_ms = kms;
     if (out_ms) *out_ms = ms;
     status_check(c, p.status.as<int>());
 }
@@ -853,8 +870,10 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
     if (!G) G = std::min<uint32_t>(K, 4);
     if (!B) B = 256;
     SweepPlan* p = g.plan;
-    const bool reuse = p && p->n == g.n && p->E == g.e_total && p->K == K && p->G == std::min(G, std::min<uint32_t>(K, 32)) &&
-                       p->block == B && p->labels == want_labels && g.edges_valid;
+    const bool reuse = p && p->n == g.n && p->E == g.e_total && p->K == K &&
+                       p->G == std::max<uint32_t>(1, std::min(G, std::min<uint32_t>(K, 32))) && p->block == B &&
+                       p->labels == want_labels && p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
+                       p->key_ptrs[2] == g.ew.p && p->key_ptrs[3] == g.dists.p && p->key_ptrs[4] == g.counts.p;
     if (!reuse) {
         if (g.plan) sweep_free(g.plan);
         g.plan = nullptr;
@@ -946,6 +965,15 @@ cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint3
         if (out_nedges) *out_nedges = r.nedges;
         if (out_ncomp) *out_ncomp = r.ncomp;
         if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_sweep_timing(cs_graph* gp, float* graph_ms, float* kernel_ms) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        if (!g->plan) fail(CS_ERR_STATE, "cs_sweep_timing: no sweep has run");
+        if (graph_ms) *graph_ms = g->plan->last_graph_ms;
+        if (kernel_ms) *kernel_ms = g->plan->last_kernel_ms;
     });
 }
 
