@@ -226,20 +226,36 @@ cs_status cs_ctx_create(int32_t device, cs_ctx** out) {
     }
 }
 
+}  // extern "C"
+
+namespace csb {
+/// Free a context's resources.  Never throws (it runs at interpreter teardown too,
+/// when the runtime may already be gone).
+void ctx_free(Ctx* c) {
+    if (cudaSetDevice(c->device) == cudaSuccess && c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& b : c->scratch) b.release();
+    c->status.release();
+    for (auto& b : c->pinned) b.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    c->stream = nullptr;
+    cudaGetLastError();
+    delete c;
+}
+}  // namespace csb
+
+extern "C" {
+
 void cs_ctx_destroy(cs_ctx* ctx) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (!c) return;
     {
         std::lock_guard<std::recursive_mutex> lk(c->mu);
-        cudaSetDevice(c->device);
-        cudaStreamSynchronize(c->stream);
-        for (auto& b : c->scratch) b.release();
-        c->status.release();
-        for (auto& b : c->pinned) b.release();
-        cudaStreamDestroy(c->stream);
-        c->stream = nullptr;
+        if (c->live_graphs > 0) {
+            c->destroy_pending = true;  // freed with its last graph
+            return;
+        }
     }
-    delete c;
+    ctx_free(c);
 }
 
 cs_status cs_ctx_trim(cs_ctx* ctx) {

@@ -78,6 +78,8 @@ struct Ctx {
     DevBuf scratch[8];      // per-call scratch, reused across calls
     PinnedBuf pinned[2];
     DevBuf status;          // device error word(s) written by bounded waits
+    int live_graphs = 0;    // graphs created on this context and not yet destroyed
+    bool destroy_pending = false;  // cs_ctx_destroy called while graphs were alive
     void bind() const;      // cudaSetDevice(device)
     void sync();            // stream synchronise + error check
 };
@@ -192,6 +194,8 @@ cs_status guarded(Ctx* c, F&& f) {
         return CS_ERR_INVALID;
     }
 }
+
+void ctx_free(Ctx* c);
 
 // launch bookkeeping
 inline void count_launch(Ctx& c, uint64_t n = 1) { c.launches += n; }

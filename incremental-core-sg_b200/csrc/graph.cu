@@ -264,6 +264,7 @@ cs_status cs_graph_create(cs_ctx* ctx, uint32_t dim, uint32_t k_max, int32_t met
             fail(CS_ERR_UNSUPPORTED, "cs_graph_create: only L2 and cosine run on the device");
         Graph* g = new Graph();
         g->ctx = c;
+        ++c->live_graphs;
         g->dim = dim;
         g->k = k_max;
         g->stride = (dim + 7u) & ~7u;
@@ -275,11 +276,17 @@ cs_status cs_graph_create(cs_ctx* ctx, uint32_t dim, uint32_t k_max, int32_t met
 void cs_graph_destroy(cs_graph* gp) {
     Graph* g = reinterpret_cast<Graph*>(gp);
     if (!g) return;
+    Ctx* c = g->ctx;
+    bool free_ctx = false;
     {
-        std::lock_guard<std::recursive_mutex> lk(g->ctx->mu);
-        g->ctx->bind();
+        std::lock_guard<std::recursive_mutex> lk(c->mu);
+        cudaSetDevice(c->device);  // no throw: may run at interpreter teardown
         delete g;
+        cudaGetLastError();
+        --c->live_graphs;
+        free_ctx = c->destroy_pending && c->live_graphs == 0;
     }
+    if (free_ctx) ctx_free(c);
 }
 
 static cs_status set_points_impl(Graph* g, const float* rows, uint64_t n, uint32_t row_stride, bool append) {

@@ -35,7 +35,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSlots = 32;         // candidate slots per node
+constexpr int kSlots = 64;         // candidate slots per node (two-choice hashed)
 constexpr int kMaxSample = 32;     // smpN ceiling (cuda/cuda_common.cuh:30)
 constexpr int kMaxNewList = 2 * kMaxSample;
 constexpr int kMaxOldList = 4 * kMaxSample;
@@ -45,7 +45,27 @@ inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(b, 1u << 30)));
 }
 
-__device__ __forceinline__ uint32_t slot_of(uint32_t id) { return (id * 2654435761u) >> 27; }  // 5 bits
+__device__ __forceinline__ uint32_t slot1(uint32_t id) { return (id * 2654435761u) >> 26; }  // 6 bits
+__device__ __forceinline__ uint32_t slot2(uint32_t id) {
+    const uint32_t a = ((id ^ 0x5BD1E995u) * 0x9E3779B1u) >> 26;
+    return a == slot1(id) ? (a ^ 1u) : a;
+}
+
+/// Offer a packed (rank, id) key to a node's candidate table: atomicMin into the
+/// id's first slot; whichever key loses there (the offer, or the key it displaced)
+/// gets one more atomicMin into its other slot.  A key equal to the slot's content
+/// is already present and stops.
+__device__ __forceinline__ void offer(unsigned long long* __restrict__ table, unsigned long long key) {
+    const uint32_t id = static_cast<uint32_t>(key);
+    const uint32_t s1 = slot1(id);
+    const unsigned long long old = atomicMin(table + s1, key);
+    if (old == key) return;
+    const unsigned long long loser = old < key ? key : old;
+    if (loser == kNoKey) return;
+    const uint32_t lid = static_cast<uint32_t>(loser);
+    const uint32_t alt = slot1(lid) == s1 ? slot2(lid) : slot1(lid);
+    atomicMin(table + alt, loser);
+}
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
@@ -132,8 +152,8 @@ __global__ void k_threshold(const float* __restrict__ rank, const uint32_t* __re
 }
 
 /// Random top-up candidates for short lists (init_random, src/nndescent.cpp:348-377):
-/// `needed + needed/2 + 4` draws per node, split into passes of at most 32 so each
-/// pass fits the candidate slots; `pass` selects the draws of this pass.
+/// `needed + needed/2 + 4` draws per node, in passes of 32 (one per lane), each
+/// followed by a merge.
 __global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_t stride,
                               const uint32_t* __restrict__ counts, uint32_t k, uint64_t seed, int pass,
                               unsigned long long* __restrict__ cand) {
@@ -150,7 +170,7 @@ __global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_
     const uint32_t cand_id = static_cast<uint32_t>((h >> 32) % n);
     if (cand_id == p) return;
     const float r = l2sqr_ref(pts + static_cast<uint64_t>(p) * stride, pts + static_cast<uint64_t>(cand_id) * stride, stride);
-    atomicMin(cand + static_cast<uint64_t>(p) * kSlots + slot_of(cand_id), make_key(r, cand_id));
+    offer(cand + static_cast<uint64_t>(p) * kSlots, make_key(r, cand_id));
 }
 
 /// Sampling + reverse publication (one warp per node).
@@ -257,8 +277,8 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
         if (u1 == u2) continue;
         const float r = l2sqr_ref(s_row + static_cast<size_t>(a) * stride, s_row + static_cast<size_t>(b) * stride, stride);
         ++my_evals;
-        if (r < s_thr[a]) atomicMin(cand + static_cast<uint64_t>(u1) * kSlots + slot_of(u2), make_key(r, u2));
-        if (r < s_thr[b]) atomicMin(cand + static_cast<uint64_t>(u2) * kSlots + slot_of(u1), make_key(r, u1));
+        if (r < s_thr[a]) offer(cand + static_cast<uint64_t>(u1) * kSlots, make_key(r, u2));
+        if (r < s_thr[b]) offer(cand + static_cast<uint64_t>(u2) * kSlots, make_key(r, u1));
     }
     if (evals) {
         for (int o = 16; o > 0; o >>= 1) my_evals += __shfl_xor_sync(0xFFFFFFFFu, my_evals, o);
@@ -266,20 +286,23 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     }
 }
 
-/// Merge candidates into the sorted lists (one warp per node).  I items per lane
-/// (a power of two): items 0..L-1 hold the list (k <= 32*L), item L this lane's
-/// candidate slot, the rest are empty padding for the bitonic network.
-template <int I, int L>
+/// Merge the candidate table into the sorted list (one warp per node).  Four items
+/// per lane (128 elements for the bitonic network): the list in items 0..L-1
+/// (k <= 32*L), the 64 candidate slots in items L, L+1 (slot j and 32+j per lane),
+/// empty padding after.  Candidates already listed, duplicated across the two
+/// slots of an id, or not better than the current k-th entry are dropped first.
+template <int L>
 __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, float* __restrict__ rank,
                         uint8_t* __restrict__ flags, uint32_t* __restrict__ counts, float* __restrict__ thr,
                         unsigned long long* __restrict__ cand, uint32_t* __restrict__ rnew_cnt,
                         uint32_t* __restrict__ rold_cnt, unsigned long long* __restrict__ updates) {
+    constexpr int I = 4;
+    static_assert(L + 2 <= I, "merge layout");
     const uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (u >= n) return;
     const unsigned lane = threadIdx.x & 31u;
-    static_assert(L + 1 <= I, "merge layout");
     unsigned long long key[I];
-    uint32_t pay[I];  // bit 0: new flag, bit 1: came from a candidate slot
+    uint32_t pay[I];  // bit 0: new flag, bit 1: came from the candidate table
     const uint32_t c = counts[u];
     const uint64_t base = static_cast<uint64_t>(u) * k;
 #pragma unroll
@@ -293,28 +316,42 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
             pay[i] = 0;
         }
     }
-    // candidate slot of this lane
-    unsigned long long ck = cand[static_cast<uint64_t>(u) * kSlots + lane];
-    cand[static_cast<uint64_t>(u) * kSlots + lane] = kNoKey;
-    const uint32_t cid = static_cast<uint32_t>(ck);
     const float kth = c >= k ? rank[base + k - 1] : __int_as_float(0x7f800000);
-    bool ok = ck != kNoKey && cid != u && cid < n;
-    if (ok) ok = __uint_as_float(static_cast<uint32_t>(ck >> 32)) < kth;
-    // drop ids already in the list
+    unsigned long long* table = cand + static_cast<uint64_t>(u) * kSlots;
+    unsigned long long ck[2];
+    bool ok[2];
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
-        const uint32_t lid = static_cast<uint32_t>(key[i]);
-        const bool lvalid = key[i] != kNoKey;
+    for (int h = 0; h < 2; ++h) {
+        ck[h] = table[h * 32 + lane];
+        table[h * 32 + lane] = kNoKey;
+        const uint32_t cid = static_cast<uint32_t>(ck[h]);
+        ok[h] = ck[h] != kNoKey && cid != u && cid < n &&
+                __uint_as_float(static_cast<uint32_t>(ck[h] >> 32)) < kth;
+    }
+    // drop ids already listed, and the second copy of a key held by two slots
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t cid = static_cast<uint32_t>(ck[h]);
+        const uint32_t my_slot = static_cast<uint32_t>(h) * 32u + lane;
         for (int t = 0; t < 32; ++t) {
-            const uint32_t other = __shfl_sync(0xFFFFFFFFu, lid, t);
-            const bool ov = __shfl_sync(0xFFFFFFFFu, lvalid, t);
-            if (ov && other == cid) ok = false;
+#pragma unroll
+            for (int i = 0; i < L; ++i) {
+                const unsigned long long lk = __shfl_sync(0xFFFFFFFFu, key[i], t);
+                if (lk != kNoKey && static_cast<uint32_t>(lk) == cid) ok[h] = false;
+            }
+            const unsigned long long o0 = __shfl_sync(0xFFFFFFFFu, ck[0], t);
+            const unsigned long long o1 = __shfl_sync(0xFFFFFFFFu, ck[1], t);
+            if (o0 == ck[h] && static_cast<uint32_t>(t) < my_slot) ok[h] = false;
+            if (o1 == ck[h] && 32u + static_cast<uint32_t>(t) < my_slot) ok[h] = false;
         }
     }
-    key[L] = ok ? ck : kNoKey;
-    pay[L] = ok ? 3u : 0u;
 #pragma unroll
-    for (int i = L + 1; i < I; ++i) {
+    for (int h = 0; h < 2; ++h) {
+        key[L + h] = ok[h] ? ck[h] : kNoKey;
+        pay[L + h] = ok[h] ? 3u : 0u;
+    }
+#pragma unroll
+    for (int i = L + 2; i < I; ++i) {
         key[i] = kNoKey;
         pay[i] = 0;
     }
@@ -337,12 +374,11 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
         cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
         inserted += __shfl_xor_sync(0xFFFFFFFFu, inserted, o);
     }
-    // k-th entry lives at element k-1
+    // the k-th entry is element k-1: lane (k-1)%32 of item (k-1)/32
     const uint32_t e = k - 1;
-    const unsigned long long kk = __shfl_sync(0xFFFFFFFFu, key[0], e & 31u);
-    unsigned long long kth_key = kk;
+    unsigned long long kth_key = kNoKey;
 #pragma unroll
-    for (int i = 1; i < I; ++i) {
+    for (int i = 0; i < I; ++i) {
         const unsigned long long x = __shfl_sync(0xFFFFFFFFu, key[i], e & 31u);
         if (static_cast<uint32_t>(i) == e / 32u) kth_key = x;
     }
@@ -364,12 +400,12 @@ void launch_merge(Ctx& c, Graph& g, KnnScratch& s, unsigned long long* updates) 
     const uint32_t n = static_cast<uint32_t>(g.n);
     const unsigned grid = static_cast<unsigned>((n + kWarps - 1) / kWarps);
     if (g.k <= 32) {
-        k_merge<2, 1><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
+        k_merge<1><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
                                                      s.cand.as<unsigned long long>(), s.rnew_cnt.as<uint32_t>(),
                                                      s.rold_cnt.as<uint32_t>(), updates);
     } else {
-        k_merge<4, 2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
+        k_merge<2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
                                                      s.cand.as<unsigned long long>(), s.rnew_cnt.as<uint32_t>(),
                                                      s.rold_cnt.as<uint32_t>(), updates);

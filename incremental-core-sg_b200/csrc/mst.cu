@@ -661,16 +661,16 @@ struct SweepPlan {
     uint64_t edges_version = 0;
     DevBuf mpts, core, parent, best, touched, wl, bitmap, bins, ctr, bar, status, tiles, lab, out, counts;
     uint32_t nbl = 0, ntl = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
     bool captured = false;
     std::vector<uint32_t> host_mpts;
     const void* key_ptrs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;  // around the persistent kernel
     float last_graph_ms = 0.0f, last_kernel_ms = 0.0f;
     ~SweepPlan() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
+        if (exec_pre) cudaGraphExecDestroy(exec_pre);
+        if (exec_main) cudaGraphExecDestroy(exec_main);
+        if (exec_post) cudaGraphExecDestroy(exec_post);
         if (ev_k0) cudaEventDestroy(ev_k0);
         if (ev_k1) cudaEventDestroy(ev_k1);
     }
@@ -707,8 +707,12 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     return a;
 }
 
-/// Enqueue the whole sweep on the context stream (captured into the plan's graph).
-void enqueue_sweep(Graph& g, SweepPlan& p) {
+/// The sweep is enqueued in three parts, each captured into its own CUDA graph:
+///   pre   reset the per-sweep state, core tables of the K mpts values
+///   main  the persistent cooperative Boruvka kernel (all K MSTs)
+///   post  labels and tree compaction
+/// so stream events between the parts time the persistent kernel alone.
+void enqueue_pre(Graph& g, SweepPlan& p) {
     Ctx& c = *g.ctx;
     const uint64_t n = p.n;
     CSB_CUDA(cudaMemsetAsync(p.status.p, 0, 64, c.stream));
@@ -721,32 +725,69 @@ void enqueue_sweep(Graph& g, SweepPlan& p) {
                                                               p.n, g.k, p.mpts.as<uint32_t>(), p.K,
                                                               p.core.as<float>());
         count_launch(c);
-        SweepArgs a = args_of(g, p);
-        void* params[] = {&a};
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(p.grid);
-        cfg.blockDim = dim3(p.block);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = c.stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        CSB_CUDA(cudaEventRecord(p.ev_k0, c.stream));
-        CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
-        CSB_CUDA(cudaEventRecord(p.ev_k1, c.stream));
-        count_launch(c);
-        if (p.labels) {
-            launch_labels(c, p.parent.as<uint32_t>(), p.n, p.K, p.lab.as<uint32_t>(), p.tiles.as<uint32_t>(),
-                          p.counts.as<unsigned long long>());
-        }
-        launch_compact(c, p.bitmap.as<uint32_t>(), p.W, p.K,
-                       p.tiles.as<uint32_t>() + static_cast<uint64_t>(p.K) * p.nbl,
-                       p.counts.as<unsigned long long>() + p.K, g.eu.as<uint32_t>(), g.ev.as<uint32_t>(),
-                       g.ew.as<float>(), p.core.as<float>(), p.n, n ? n - 1 : 0, p.out.as<cs_edge>(),
-                       p.status.as<int>());
     }
+}
+
+void enqueue_main(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    if (!p.n) return;
+    SweepArgs a = args_of(g, p);
+    void* params[] = {&a};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.grid);
+    cfg.blockDim = dim3(p.block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
+    count_launch(c);
+}
+
+void enqueue_post(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    const uint64_t n = p.n;
+    if (!n) return;
+    if (p.labels) {
+        launch_labels(c, p.parent.as<uint32_t>(), p.n, p.K, p.lab.as<uint32_t>(), p.tiles.as<uint32_t>(),
+                      p.counts.as<unsigned long long>());
+    }
+    launch_compact(c, p.bitmap.as<uint32_t>(), p.W, p.K, p.tiles.as<uint32_t>() + static_cast<uint64_t>(p.K) * p.nbl,
+                   p.counts.as<unsigned long long>() + p.K, g.eu.as<uint32_t>(), g.ev.as<uint32_t>(), g.ew.as<float>(),
+                   p.core.as<float>(), p.n, n - 1, p.out.as<cs_edge>(), p.status.as<int>());
+}
+
+using Enqueue = void (*)(Graph&, SweepPlan&);
+
+/// Capture one part into a graph; false (and no graph) when capture is refused.
+bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
+    Ctx& c = *g.ctx;
+    *out = nullptr;
+    if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const uint64_t before = c.launches;
+    bool ok = true;
+    try {
+        f(g, p);
+    } catch (...) {
+        ok = false;
+    }
+    c.launches = before;  // counted when replayed
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+    ok = ok && e == cudaSuccess && graph;
+    if (ok) ok = cudaGraphInstantiate(out, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        cudaGetLastError();
+        *out = nullptr;
+    }
+    return ok;
 }
 
 SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labels) {
@@ -791,28 +832,10 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labe
         CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep, static_cast<int>(block), 0));
         if (occ < 1) fail(CS_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
         p->grid = static_cast<uint32_t>(c.sm_count) * static_cast<uint32_t>(occ);
-        // capture the sweep into a CUDA graph
-        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-        CSB_CUDA(cudaStreamIsCapturing(c.stream, &cs));
-        bool ok = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-        if (ok) {
-            const uint64_t before = c.launches;
-            try {
-                enqueue_sweep(g, *p);
-            } catch (...) {
-                cudaGraph_t junk = nullptr;
-                cudaStreamEndCapture(c.stream, &junk);
-                if (junk) cudaGraphDestroy(junk);
-                cudaGetLastError();
-                ok = false;
-            }
-            c.launches = before;  // counted when replayed
-            if (ok) {
-                ok = cudaStreamEndCapture(c.stream, &p->graph) == cudaSuccess && p->graph;
-                if (ok) ok = cudaGraphInstantiate(&p->exec, p->graph, 0) == cudaSuccess;
-            }
-            if (!ok) cudaGetLastError();
-        }
+        // capture the three parts into CUDA graphs (replayed by run_plan)
+        bool ok = capture_part(g, *p, enqueue_pre, &p->exec_pre);
+        ok = capture_part(g, *p, enqueue_main, &p->exec_main) && ok;
+        ok = capture_part(g, *p, enqueue_post, &p->exec_post) && ok;
         p->captured = ok;
     } catch (...) {
         delete p;
@@ -821,7 +844,8 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labe
     return p;
 }
 
-uint64_t kernels_per_sweep(const SweepPlan& p) { return p.n ? (1 + 1 + (p.labels ? 4 : 0) + 3) : 0; }
+uint64_t kernels_pre(const SweepPlan& p) { return p.n ? 1 : 0; }
+uint64_t kernels_post(const SweepPlan& p) { return p.n ? ((p.labels ? 4 : 0) + 3) : 0; }
 
 void run_plan(Graph& g, SweepPlan& p, float* out_ms) {
     Ctx& c = *g.ctx;
@@ -830,17 +854,31 @@ void run_plan(Graph& g, SweepPlan& p, float* out_ms) {
     CSB_CUDA(cudaEventCreate(&e1));
     CSB_CUDA(cudaMemcpyAsync(p.mpts.p, p.host_mpts.data(), p.K * 4, cudaMemcpyHostToDevice, c.stream));
     CSB_CUDA(cudaEventRecord(e0, c.stream));
-    if (p.captured) {
-        CSB_CUDA(cudaGraphLaunch(p.exec, c.stream));
-        count_launch(c, kernels_per_sweep(p));
+    if (p.exec_pre) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_pre, c.stream));
+        count_launch(c, kernels_pre(p));
     } else {
-        enqueue_sweep(g, p);
+        enqueue_pre(g, p);
+    }
+    CSB_CUDA(cudaEventRecord(p.ev_k0, c.stream));
+    if (p.exec_main) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_main, c.stream));
+        count_launch(c, p.n ? 1 : 0);
+    } else {
+        enqueue_main(g, p);
+    }
+    CSB_CUDA(cudaEventRecord(p.ev_k1, c.stream));
+    if (p.exec_post) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_post, c.stream));
+        count_launch(c, kernels_post(p));
+    } else {
+        enqueue_post(g, p);
     }
     CSB_CUDA(cudaEventRecord(e1, c.stream));
     CSB_CUDA(cudaEventSynchronize(e1));
     float ms = 0.0f, kms = 0.0f;
     CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (p.n) CSB_CUDA(cudaEventElapsedTime(&kms, p.ev_k0, p.ev_k1));
+    CSB_CUDA(cudaEventElapsedTime(&kms, p.ev_k0, p.ev_k1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     p.last_graph_ms = ms;
