@@ -35,7 +35,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSlots = 64;         // candidate slots per node (two-choice hashed)
+constexpr int kSlots = 64;         // overflow table slots per node (two-choice hashed)
+constexpr int kCap = 128;          // append buffer per node
 constexpr int kMaxSample = 32;     // smpN ceiling (cuda/cuda_common.cuh:30)
 constexpr int kMaxNewList = 2 * kMaxSample;
 constexpr int kMaxOldList = 4 * kMaxSample;
@@ -51,11 +52,10 @@ __device__ __forceinline__ uint32_t slot2(uint32_t id) {
     return a == slot1(id) ? (a ^ 1u) : a;
 }
 
-/// Offer a packed (rank, id) key to a node's candidate table: atomicMin into the
-/// id's first slot; whichever key loses there (the offer, or the key it displaced)
-/// gets one more atomicMin into its other slot.  A key equal to the slot's content
-/// is already present and stops.
-__device__ __forceinline__ void offer(unsigned long long* __restrict__ table, unsigned long long key) {
+/// Overflow table: atomicMin into the id's first slot; whichever key loses there
+/// (the offer, or the key it displaced) gets one more atomicMin into its other
+/// slot.  A key equal to the slot's content is already present and stops.
+__device__ __forceinline__ void offer_table(unsigned long long* __restrict__ table, unsigned long long key) {
     const uint32_t id = static_cast<uint32_t>(key);
     const uint32_t s1 = slot1(id);
     const unsigned long long old = atomicMin(table + s1, key);
@@ -65,6 +65,23 @@ __device__ __forceinline__ void offer(unsigned long long* __restrict__ table, un
     const uint32_t lid = static_cast<uint32_t>(loser);
     const uint32_t alt = slot1(lid) == s1 ? slot2(lid) : slot1(lid);
     atomicMin(table + alt, loser);
+}
+
+/// Offer a packed (rank, id) key to node u: the first kCap offers of a round are
+/// appended to u's buffer as they come, later ones go to the overflow table (so
+/// the best of the overflow still has a slot).
+struct CandStore {
+    unsigned long long* buf;    // [n][kCap]
+    uint32_t* cnt;              // [n]
+    unsigned long long* table;  // [n][kSlots]
+};
+__device__ __forceinline__ void offer(const CandStore& cs, uint32_t u, unsigned long long key) {
+    const uint32_t pos = atomicAdd(cs.cnt + u, 1u);
+    if (pos < kCap) {
+        cs.buf[static_cast<uint64_t>(u) * kCap + pos] = key;
+    } else {
+        offer_table(cs.table + static_cast<uint64_t>(u) * kSlots, key);
+    }
 }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
@@ -156,7 +173,7 @@ __global__ void k_threshold(const float* __restrict__ rank, const uint32_t* __re
 /// followed by a merge.
 __global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_t stride,
                               const uint32_t* __restrict__ counts, uint32_t k, uint64_t seed, int pass,
-                              unsigned long long* __restrict__ cand) {
+                              CandStore cand) {
     const uint32_t p = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (p >= n || n < 2) return;
     const unsigned lane = threadIdx.x & 31u;
@@ -170,7 +187,7 @@ __global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_
     const uint32_t cand_id = static_cast<uint32_t>((h >> 32) % n);
     if (cand_id == p) return;
     const float r = l2sqr_ref(pts + static_cast<uint64_t>(p) * stride, pts + static_cast<uint64_t>(cand_id) * stride, stride);
-    offer(cand + static_cast<uint64_t>(p) * kSlots, make_key(r, cand_id));
+    offer(cand, p, make_key(r, cand_id));
 }
 
 /// Sampling + reverse publication (one warp per node).
@@ -229,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
                                                    const uint32_t* __restrict__ rnew, const uint32_t* __restrict__ rold,
                                                    const uint32_t* __restrict__ rnew_cnt,
                                                    const uint32_t* __restrict__ rold_cnt, const float* __restrict__ thr,
-                                                   unsigned long long* __restrict__ cand, int warps_per_block,
+                                                   CandStore cand, int warps_per_block,
                                                    unsigned long long* __restrict__ evals) {
     extern __shared__ float smem[];
     const int w = threadIdx.x >> 5;
@@ -277,8 +294,8 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
         if (u1 == u2) continue;
         const float r = l2sqr_ref(s_row + static_cast<size_t>(a) * stride, s_row + static_cast<size_t>(b) * stride, stride);
         ++my_evals;
-        if (r < s_thr[a]) offer(cand + static_cast<uint64_t>(u1) * kSlots, make_key(r, u2));
-        if (r < s_thr[b]) offer(cand + static_cast<uint64_t>(u2) * kSlots, make_key(r, u1));
+        if (r < s_thr[a]) offer(cand, u1, make_key(r, u2));
+        if (r < s_thr[b]) offer(cand, u2, make_key(r, u1));
     }
     if (evals) {
         for (int o = 16; o > 0; o >>= 1) my_evals += __shfl_xor_sync(0xFFFFFFFFu, my_evals, o);
@@ -286,29 +303,30 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     }
 }
 
-/// Merge the candidate table into the sorted list (one warp per node).  Four items
-/// per lane (128 elements for the bitonic network): the list in items 0..L-1
-/// (k <= 32*L), the 64 candidate slots in items L, L+1 (slot j and 32+j per lane),
-/// empty padding after.  Candidates already listed, duplicated across the two
-/// slots of an id, or not better than the current k-th entry are dropped first.
-template <int L>
+/// Merge a node's offers into its sorted list (one warp per node).  The offers
+/// (the append buffer, then the overflow table when it was used) are taken 32 at a
+/// time: each chunk drops invalid keys, ids already listed, keys repeated inside the
+/// chunk and keys not better than the current k-th entry, and if anything is left
+/// the list (LI items per lane) and the chunk are sorted together by a warp bitonic
+/// network of I = 2*LI... elements and the first k kept.  Newcomers carry the new
+/// flag; the ones still listed at the end are the round's updates.
+template <int LI, int I>
 __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, float* __restrict__ rank,
                         uint8_t* __restrict__ flags, uint32_t* __restrict__ counts, float* __restrict__ thr,
-                        unsigned long long* __restrict__ cand, uint32_t* __restrict__ rnew_cnt,
-                        uint32_t* __restrict__ rold_cnt, unsigned long long* __restrict__ updates) {
-    constexpr int I = 4;
-    static_assert(L + 2 <= I, "merge layout");
+                        CandStore cand, uint32_t* __restrict__ rnew_cnt, uint32_t* __restrict__ rold_cnt,
+                        unsigned long long* __restrict__ updates) {
+    static_assert(LI + 1 <= I, "merge layout");
     const uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (u >= n) return;
     const unsigned lane = threadIdx.x & 31u;
     unsigned long long key[I];
-    uint32_t pay[I];  // bit 0: new flag, bit 1: came from the candidate table
+    uint32_t pay[I];  // bit 0: new flag, bit 1: came from an offer
     const uint32_t c = counts[u];
     const uint64_t base = static_cast<uint64_t>(u) * k;
 #pragma unroll
-    for (int i = 0; i < L; ++i) {
+    for (int i = 0; i < I; ++i) {
         const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
-        if (j < c) {
+        if (i < LI && j < c) {
             key[i] = make_key(rank[base + j], ids[base + j]);
             pay[i] = flags[base + j] ? 1u : 0u;
         } else {
@@ -316,50 +334,77 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
             pay[i] = 0;
         }
     }
-    const float kth = c >= k ? rank[base + k - 1] : __int_as_float(0x7f800000);
-    unsigned long long* table = cand + static_cast<uint64_t>(u) * kSlots;
-    unsigned long long ck[2];
-    bool ok[2];
+    const uint32_t offered = cand.cnt[u];
+    const uint32_t nbuf = min(offered, static_cast<uint32_t>(kCap));
+    const bool table_used = offered > static_cast<uint32_t>(kCap);
+    const uint32_t total = nbuf + (table_used ? kSlots : 0);
+    const unsigned long long* bufp = cand.buf + static_cast<uint64_t>(u) * kCap;
+    unsigned long long* tabp = cand.table + static_cast<uint64_t>(u) * kSlots;
+    // k-th key of the current list (element k-1)
+    auto kth_of = [&]() -> unsigned long long {
+        const uint32_t e = k - 1;
+        unsigned long long x = kNoKey;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        ck[h] = table[h * 32 + lane];
-        table[h * 32 + lane] = kNoKey;
-        const uint32_t cid = static_cast<uint32_t>(ck[h]);
-        ok[h] = ck[h] != kNoKey && cid != u && cid < n &&
-                __uint_as_float(static_cast<uint32_t>(ck[h] >> 32)) < kth;
-    }
-    // drop ids already listed, and the second copy of a key held by two slots
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const uint32_t cid = static_cast<uint32_t>(ck[h]);
-        const uint32_t my_slot = static_cast<uint32_t>(h) * 32u + lane;
-        for (int t = 0; t < 32; ++t) {
-#pragma unroll
-            for (int i = 0; i < L; ++i) {
-                const unsigned long long lk = __shfl_sync(0xFFFFFFFFu, key[i], t);
-                if (lk != kNoKey && static_cast<uint32_t>(lk) == cid) ok[h] = false;
-            }
-            const unsigned long long o0 = __shfl_sync(0xFFFFFFFFu, ck[0], t);
-            const unsigned long long o1 = __shfl_sync(0xFFFFFFFFu, ck[1], t);
-            if (o0 == ck[h] && static_cast<uint32_t>(t) < my_slot) ok[h] = false;
-            if (o1 == ck[h] && 32u + static_cast<uint32_t>(t) < my_slot) ok[h] = false;
+        for (int i = 0; i < I; ++i) {
+            const unsigned long long y = __shfl_sync(0xFFFFFFFFu, key[i], e & 31u);
+            if (static_cast<uint32_t>(i) == e / 32u) x = y;
         }
-    }
+        return x;
+    };
+    unsigned long long kth = kth_of();
+    for (uint32_t off = 0; off < total; off += 32) {
+        const uint32_t t = off + lane;
+        unsigned long long ck = kNoKey;
+        if (t < total) {
+            if (t < nbuf) {
+                ck = bufp[t];
+            } else {
+                ck = tabp[t - nbuf];
+                tabp[t - nbuf] = kNoKey;  // the table is reset as it is read
+            }
+        }
+        const uint32_t cid = static_cast<uint32_t>(ck);
+        // kth's rank bits compare like the key's (ids only break exact ties, where a
+        // newcomer does not displace: the reference inserts behind equal distances)
+        bool ok = ck != kNoKey && cid != u && cid < n &&
+                  (kth == kNoKey || static_cast<uint32_t>(ck >> 32) < static_cast<uint32_t>(kth >> 32));
+        // repeated inside the chunk: keep the lowest lane holding the key
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, ck);
+        if (static_cast<int>(lane) != __ffs(same) - 1) ok = false;
+        // already listed
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        key[L + h] = ok[h] ? ck[h] : kNoKey;
-        pay[L + h] = ok[h] ? 3u : 0u;
-    }
+        for (int i = 0; i < LI; ++i) {
+            const uint32_t lid = static_cast<uint32_t>(key[i]);
+            const bool lv = key[i] != kNoKey;
+            for (int q = 0; q < 32; ++q) {
+                const uint32_t other = __shfl_sync(0xFFFFFFFFu, lid, q);
+                const bool ov = __shfl_sync(0xFFFFFFFFu, lv, q);
+                if (ov && other == cid) ok = false;
+            }
+        }
+        if (!__any_sync(0xFFFFFFFFu, ok)) continue;
+        key[LI] = ok ? ck : kNoKey;
+        pay[LI] = ok ? 3u : 0u;
 #pragma unroll
-    for (int i = L + 2; i < I; ++i) {
-        key[i] = kNoKey;
-        pay[i] = 0;
+        for (int i = LI + 1; i < I; ++i) {
+            key[i] = kNoKey;
+            pay[i] = 0;
+        }
+        warp_bitonic<I>(key, pay);
+        // keep the first k; drop the rest
+#pragma unroll
+        for (int i = 0; i < I; ++i) {
+            const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
+            if (j >= k) {
+                key[i] = kNoKey;
+                pay[i] = 0;
+            }
+        }
+        kth = kth_of();
     }
-    warp_bitonic<I>(key, pay);
-    // the first k elements (e = i*32 + lane < k) are the new list
     uint32_t inserted = 0, cnt = 0;
 #pragma unroll
-    for (int i = 0; i < I; ++i) {
+    for (int i = 0; i < LI; ++i) {
         const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
         if (j < k) {
             const bool valid = key[i] != kNoKey;
@@ -374,18 +419,11 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
         cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
         inserted += __shfl_xor_sync(0xFFFFFFFFu, inserted, o);
     }
-    // the k-th entry is element k-1: lane (k-1)%32 of item (k-1)/32
-    const uint32_t e = k - 1;
-    unsigned long long kth_key = kNoKey;
-#pragma unroll
-    for (int i = 0; i < I; ++i) {
-        const unsigned long long x = __shfl_sync(0xFFFFFFFFu, key[i], e & 31u);
-        if (static_cast<uint32_t>(i) == e / 32u) kth_key = x;
-    }
     if (lane == 0) {
         counts[u] = cnt;
-        thr[u] = (cnt >= k && kth_key != kNoKey) ? __uint_as_float(static_cast<uint32_t>(kth_key >> 32))
-                                                 : __int_as_float(0x7f800000);
+        thr[u] = (cnt >= k && kth != kNoKey) ? __uint_as_float(static_cast<uint32_t>(kth >> 32))
+                                             : __int_as_float(0x7f800000);
+        cand.cnt[u] = 0;
         rnew_cnt[u] = 0;
         rold_cnt[u] = 0;
         if (inserted && updates) atomicAdd(updates, static_cast<unsigned long long>(inserted));
@@ -393,21 +431,29 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
 }
 
 struct KnnScratch {
-    DevBuf thr, cand, new_s, old_s, ns, nold, rnew, rold, rnew_cnt, rold_cnt, counters;
+    DevBuf thr, cand, cand_buf, cand_cnt, new_s, old_s, ns, nold, rnew, rold, rnew_cnt, rold_cnt, counters;
 };
+
+CandStore store_of(KnnScratch& s) {
+    CandStore cs;
+    cs.buf = s.cand_buf.as<unsigned long long>();
+    cs.cnt = s.cand_cnt.as<uint32_t>();
+    cs.table = s.cand.as<unsigned long long>();
+    return cs;
+}
 
 void launch_merge(Ctx& c, Graph& g, KnnScratch& s, unsigned long long* updates) {
     const uint32_t n = static_cast<uint32_t>(g.n);
     const unsigned grid = static_cast<unsigned>((n + kWarps - 1) / kWarps);
     if (g.k <= 32) {
-        k_merge<1><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
+        k_merge<1, 2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
-                                                     s.cand.as<unsigned long long>(), s.rnew_cnt.as<uint32_t>(),
+                                                     store_of(s), s.rnew_cnt.as<uint32_t>(),
                                                      s.rold_cnt.as<uint32_t>(), updates);
     } else {
-        k_merge<2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
+        k_merge<2, 4><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
-                                                     s.cand.as<unsigned long long>(), s.rnew_cnt.as<uint32_t>(),
+                                                     store_of(s), s.rnew_cnt.as<uint32_t>(),
                                                      s.rold_cnt.as<uint32_t>(), updates);
     }
     count_launch(c);
@@ -431,6 +477,8 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
     KnnScratch s;
     s.thr.ensure(n * 4ull);
     s.cand.ensure(n * 8ull * kSlots);
+    s.cand_buf.ensure(n * 8ull * kCap);
+    s.cand_cnt.ensure(n * 4ull);
     s.new_s.ensure(n * 4ull * kMaxSample);
     s.old_s.ensure(n * 4ull * 3 * kMaxSample);
     s.ns.ensure(n * 4ull);
@@ -443,6 +491,7 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
     unsigned long long* d_updates = s.counters.as<unsigned long long>();
     unsigned long long* d_evals = d_updates + 1;
     CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
+    CSB_CUDA(cudaMemsetAsync(s.cand_cnt.p, 0, n * 4ull, c.stream));
     CSB_CUDA(cudaMemsetAsync(s.rnew_cnt.p, 0, n * 4ull, c.stream));
     CSB_CUDA(cudaMemsetAsync(s.rold_cnt.p, 0, n * 4ull, c.stream));
     CSB_CUDA(cudaMemsetAsync(s.counters.p, 0, 64, c.stream));
@@ -455,7 +504,7 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
         const uint32_t max_attempts = k + k / 2 + 4;
         for (int pass = 0; pass * 32u < max_attempts; ++pass) {
             k_random_push<<<gw, kThreads, 0, c.stream>>>(g.pts.as<float>(), n, g.stride, g.counts.as<uint32_t>(), k,
-                                                          seed, pass, s.cand.as<unsigned long long>());
+                                                          seed, pass, store_of(s));
             count_launch(c);
             launch_merge(c, g, s, nullptr);
         }
@@ -482,7 +531,7 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
                                                   s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
                                                   s.rnew.as<uint32_t>(), s.rold.as<uint32_t>(),
                                                   s.rnew_cnt.as<uint32_t>(), s.rold_cnt.as<uint32_t>(),
-                                                  s.thr.as<float>(), s.cand.as<unsigned long long>(), wpb, d_evals);
+                                                  s.thr.as<float>(), store_of(s), wpb, d_evals);
         count_launch(c, 2);
         launch_merge(c, g, s, d_updates);
         check_launch(c, "NN-Descent round");
