@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--group", type=int, default=0, help="sweep group size (0: autotune)")
+    ap.add_argument("--block", type=int, default=0, help="sweep block size (0: autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -244,7 +246,11 @@ def main():
     log(f"[rank {rank}] build {build_s:.3f}s {st} |E|={E}")
 
     # ---- batched sweep
-    group, block = g.autotune(mpts)
+    if args.group and args.block:
+        group, block = args.group, args.block
+        g.set_sweep_shape(group, block)
+    else:
+        group, block = g.autotune(mpts)
     log(f"[rank {rank}] autotuned group={group} block={block}")
     for _ in range(args.warmup):
         g.sweep_device(mpts)
