@@ -208,6 +208,30 @@ cs_status cs_set_sweep_shape(cs_graph* g, uint32_t group, uint32_t block_threads
 cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_group,
                             uint32_t* out_block);
 
+/* ---- allocation-free MST (no counterpart in the reference) ------------------- */
+
+/* MST of a caller-provided edge list that allocates nothing, for callers that
+ * cannot allocate device memory themselves or through a library: plugins whose
+ * host application owns every device allocation, and code that must not touch the
+ * allocation API.  Inputs and outputs are the caller's device buffers: d_u, d_v,
+ * d_w (m edges, structure of arrays), d_out_edges (n-1 edges), d_out_labels (n,
+ * optional); the scalars go to host memory (optional).  All scratch lives in one
+ * fixed 12 MiB __device__ array of this library, held by every GPU that loads the
+ * library until the process exits; limits: n <= 131072 nodes, m <= 1048576 edges,
+ * larger sizes are rejected with CS_ERR_INVALID.  Runs on the current device and
+ * `stream` (a cudaStream_t; NULL is the default stream); needs no cs_ctx; errors
+ * via cs_last_error(NULL).  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) and should come before any stream capture.  Every
+ * call reuses the same array (its contents are re-initialised per call), so calls
+ * that overlap on the GPU -- from two streams or two host threads on one device --
+ * race: serialise them.  Same result as cs_extract on the same edges: the unique
+ * minimum spanning forest under (weight bits, edge index), tree in ascending edge
+ * index order, dense labels by smallest node, exact total weight. */
+cs_status cs_mst_noalloc(const uint32_t* d_u, const uint32_t* d_v, const float* d_w, uint64_t m,
+                         uint32_t n, cs_edge* d_out_edges, uint32_t* d_out_labels,
+                         uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

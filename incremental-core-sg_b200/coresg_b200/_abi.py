@@ -70,6 +70,7 @@ _SIGS = {
     "cs_sweep_timing": (_i32, [_p, _p, _p]),
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
+    "cs_mst_noalloc": (_i32, [_p, _p, _p, _u64, _u32, _p, _p, _p, _p, _p, _p]),
 }
 
 _lib = None

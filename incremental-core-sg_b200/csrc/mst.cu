@@ -1067,3 +1067,180 @@ cs_status cs_autotune_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, uint
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Allocation-free MST entry point (cs_mst_noalloc)
+// ============================================================================
+//
+// For callers that cannot allocate device memory themselves or let a library do it:
+// plugins whose host application owns every device allocation (a fixed memory pool
+// or arena handed out by the host), and code that runs where the allocation API
+// must not be touched.  The caller passes the edge list and the output buffers as
+// device pointers; every intermediate the Boruvka rounds need lives in one
+// file-scope __device__ array of fixed size, which each GPU that loads this library
+// holds until the process exits.  No cudaMalloc, cudaFree, pinned allocation or
+// context object is involved.
+//
+// The same kernels as the plain per-mpts path (k_iota, k_phase_a, k_phase_b, the
+// label and compaction kernels) run on the caller's stream, so the result is the
+// same tree: the unique minimum spanning forest under (weight bits, edge index).
+namespace csb {
+namespace {
+
+constexpr uint32_t kNoAllocMaxNodes = 131072;   // n limit
+constexpr uint64_t kNoAllocMaxEdges = 1048576;  // m limit
+constexpr size_t kNoAllocScratchBytes = size_t(12) << 20;  // 12 MiB per GPU
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+/// Device address of the scratch array on the current device.  The first call on
+/// a device looks it up with cudaGetSymbolAddress (with that device current) and
+/// caches it; later calls only read the cache.
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) fail(CS_ERR_UNSUPPORTED, "cs_mst_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) {
+            cudaGetLastError();
+            fail(CS_ERR_CUDA, std::string("cs_mst_noalloc: cudaGetSymbolAddress of the scratch array failed: ") +
+                                  cudaGetErrorString(e));
+        }
+        g_noalloc_addr[device] = static_cast<unsigned char*>(ptr);
+    }
+    return g_noalloc_addr[device];
+}
+
+struct Carver {
+    unsigned char* base;
+    size_t off = 0;
+    template <typename T>
+    T* take(uint64_t count) {
+        off = (off + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += static_cast<size_t>(count) * sizeof(T);
+        return p;
+    }
+};
+
+/// Bytes the carve below needs for n nodes and m edges.
+size_t noalloc_bytes(uint32_t n, uint64_t m) {
+    const uint64_t W = m / 32 + 1;
+    const uint64_t nbl = blocks_for(n), ntl = std::max<uint64_t>(1, (W + kTileWords - 1) / kTileWords);
+    const uint64_t parts[] = {n * 4ull, n * 8ull, n * 4ull, std::max<uint64_t>(m, 1) * 4, std::max<uint64_t>(m, 1) * 4,
+                              W * 4, 256 * 8, 64, 64, 64, (nbl + ntl + 2) * 4};
+    size_t total = 0;
+    for (uint64_t p : parts) total = ((total + 255) & ~size_t(255)) + p;
+    return total;
+}
+
+static_assert(kNoAllocMaxNodes % 256 == 0, "limit");
+
+}  // namespace
+}  // namespace csb
+
+extern "C" cs_status cs_mst_noalloc(const uint32_t* d_u, const uint32_t* d_v, const float* d_w, uint64_t m,
+                                    uint32_t n, cs_edge* d_out_edges, uint32_t* d_out_labels, uint64_t* out_nedges,
+                                    uint32_t* out_ncomp, double* out_weight, void* stream) {
+    using namespace csb;
+    try {
+        if (n > kNoAllocMaxNodes)
+            fail(CS_ERR_INVALID, "cs_mst_noalloc: n = " + std::to_string(n) + " exceeds the limit of " +
+                                     std::to_string(kNoAllocMaxNodes) + " nodes");
+        if (m > kNoAllocMaxEdges)
+            fail(CS_ERR_INVALID, "cs_mst_noalloc: m = " + std::to_string(m) + " exceeds the limit of " +
+                                     std::to_string(kNoAllocMaxEdges) + " edges");
+        if (noalloc_bytes(n, m) > kNoAllocScratchBytes) fail(CS_ERR_INVALID, "cs_mst_noalloc: scratch too small");
+        if (m > 0 && (!d_u || !d_v || !d_w)) fail(CS_ERR_INVALID, "cs_mst_noalloc: null edge array");
+        if (n > 1 && !d_out_edges) fail(CS_ERR_INVALID, "cs_mst_noalloc: null output edge buffer");
+        if (n == 0) {
+            if (out_nedges) *out_nedges = 0;
+            if (out_ncomp) *out_ncomp = 0;
+            if (out_weight) *out_weight = 0.0;
+            return CS_OK;
+        }
+        int device = 0;
+        CSB_CUDA(cudaGetDevice(&device));
+        Carver cv{noalloc_scratch(device)};
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // a stack Ctx only carries the stream to the shared launch helpers; it owns
+        // no device memory
+        Ctx tmp;
+        tmp.device = device;
+        tmp.stream = s;
+        const uint32_t W = static_cast<uint32_t>(m / 32) + 1;
+        const uint32_t nbl = blocks_for(n);
+        const uint32_t ntl = std::max<uint32_t>(1, (W + kTileWords - 1) / kTileWords);
+        MstView mv;
+        mv.parent = cv.take<uint32_t>(n);
+        mv.best = cv.take<unsigned long long>(n);
+        mv.touched = cv.take<uint32_t>(n);
+        mv.wl0 = cv.take<uint32_t>(std::max<uint64_t>(m, 1));
+        mv.wl1 = cv.take<uint32_t>(std::max<uint64_t>(m, 1));
+        mv.bitmap = cv.take<uint32_t>(W);
+        mv.bins = cv.take<unsigned long long>(256);
+        mv.ctr = cv.take<uint32_t>(16);
+        mv.core = nullptr;
+        int* status = cv.take<int>(16);
+        unsigned long long* counts = cv.take<unsigned long long>(8);
+        uint32_t* tiles = cv.take<uint32_t>(static_cast<uint64_t>(nbl) + ntl + 2);
+        // the array keeps the previous call's contents: reset what must start empty
+        CSB_CUDA(cudaMemsetAsync(mv.best, 0xFF, static_cast<size_t>(n) * 8, s));
+        CSB_CUDA(cudaMemsetAsync(mv.bitmap, 0, static_cast<size_t>(W) * 4, s));
+        CSB_CUDA(cudaMemsetAsync(mv.bins, 0, 256 * 8, s));
+        CSB_CUDA(cudaMemsetAsync(mv.ctr, 0, 64, s));
+        CSB_CUDA(cudaMemsetAsync(status, 0, 64, s));
+        CSB_CUDA(cudaMemsetAsync(counts, 0, 64, s));
+        k_iota<<<blocks_for(n), kThreads, 0, s>>>(mv.parent, n, n);
+        int sms = 148;
+        CSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        const unsigned grid_cap = static_cast<unsigned>(sms) * 8u;
+        uint32_t in_count = static_cast<uint32_t>(m);
+        uint32_t hc[4];
+        int r = 0;
+        for (; r < kMaxRounds; ++r) {
+            if (r <= 1) in_count = static_cast<uint32_t>(m);
+            k_phase_a<<<std::min<unsigned>(grid_cap, blocks_for(in_count)), kThreads, 0, s>>>(mv, d_u, d_v, d_w, n,
+                                                                                             in_count, r);
+            CSB_CUDA(cudaGetLastError());
+            CSB_CUDA(cudaMemcpyAsync(hc, mv.ctr, sizeof(hc), cudaMemcpyDeviceToHost, s));
+            CSB_CUDA(cudaStreamSynchronize(s));
+            const uint32_t tcount = hc[2 + (r & 1)];
+            if (tcount == 0) break;
+            k_phase_b<<<std::min<unsigned>(grid_cap, blocks_for(tcount)), kThreads, 0, s>>>(mv, d_u, d_v, tcount, status);
+            CSB_CUDA(cudaGetLastError());
+            in_count = hc[(r + 1) & 1];
+            CSB_CUDA(cudaMemsetAsync(mv.ctr + (r & 1), 0, 4, s));
+            CSB_CUDA(cudaMemsetAsync(mv.ctr + 2 + ((r + 1) & 1), 0, 4, s));
+        }
+        if (r == kMaxRounds) fail(CS_ERR_TIMEOUT, "cs_mst_noalloc: Boruvka round limit reached");
+        if (d_out_labels) launch_labels(tmp, mv.parent, n, 1, d_out_labels, tiles, counts);
+        launch_compact(tmp, mv.bitmap, W, 1, tiles + nbl + 1, counts + 1, d_u, d_v, d_w, nullptr, n, n - 1,
+                       d_out_edges, status);
+        CSB_CUDA(cudaGetLastError());
+        int st = 0;
+        unsigned long long hcount[2] = {0, 0};
+        uint64_t hbins[256];
+        CSB_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CSB_CUDA(cudaMemcpyAsync(hcount, counts, sizeof(hcount), cudaMemcpyDeviceToHost, s));
+        CSB_CUDA(cudaMemcpyAsync(hbins, mv.bins, sizeof(hbins), cudaMemcpyDeviceToHost, s));
+        CSB_CUDA(cudaStreamSynchronize(s));
+        if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "cs_mst_noalloc: a union retry loop ran out");
+        if (st & kStatusCapacity) fail(CS_ERR_STATE, "cs_mst_noalloc: tree larger than n-1 edges");
+        if (out_nedges) *out_nedges = hcount[1];
+        if (out_ncomp) *out_ncomp = static_cast<uint32_t>(n - hcount[1]);
+        if (out_weight) *out_weight = exact_sum_from_bins(hbins);
+        return CS_OK;
+    } catch (const Error& e) {
+        set_thread_error(e.what());
+        return e.status;
+    } catch (const std::exception& e) {
+        set_thread_error(e.what());
+        return CS_ERR_INVALID;
+    }
+}
