@@ -182,11 +182,11 @@ cs_status cs_extract(cs_graph* g, uint32_t mpts, cs_edge* out_edges, uint32_t* o
                      uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
 
 /* The batched sweep: K MSTs (one per entry of mpts[]) from the one resident edge
- * list, reweighted on the fly and solved by one persistent cooperative launch
- * replayed from a CUDA graph (CoreSG::all_msts, src/coresg.cpp:412-417, which the
- * reference runs as K independent extractions).  Per-MST results as cs_extract,
- * packed: out_edges K*(n-1), out_labels K*n, and K-long count/weight arrays.  Any
- * output may be NULL. */
+ * list, reweighted on the fly and solved by one persistent cooperative launch per
+ * pass of up to 32 MSTs (one warp lane per MST), replayed from CUDA graphs
+ * (CoreSG::all_msts, src/coresg.cpp:412-417, which the reference runs as K
+ * independent extractions).  Per-MST results as cs_extract, packed: out_edges
+ * K*(n-1), out_labels K*n, and K-long count/weight arrays.  Any output may be NULL. */
 cs_status cs_extract_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
                            uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
                            double* out_weight);
@@ -202,10 +202,14 @@ cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32
  * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
 cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
 
-/* Sweep tuning knobs (group size = MSTs solved concurrently, block size); 0 picks
- * the cached autotuned value. */
-cs_status cs_set_sweep_shape(cs_graph* g, uint32_t group, uint32_t block_threads);
-cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_group,
+/* Sweep tuning knobs.  flatten_div: the union-find forests are flattened between
+ * Boruvka rounds when the next round's worklist exceeds n / flatten_div
+ * (0xFFFFFFFF: never); block_threads: 128, 256 or 512.  0 picks the value cached by
+ * cs_autotune_sweep for this (n, |E|, K, SM count), else the defaults (4, 512). */
+cs_status cs_set_sweep_shape(cs_graph* g, uint32_t flatten_div, uint32_t block_threads);
+/* Project-written autotuner: times every (block, flatten_div) pair on the resident
+ * graph and caches the fastest for later sweeps of this shape. */
+cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_flatten,
                             uint32_t* out_block);
 
 /* ---- allocation-free MST (no counterpart in the reference) ------------------- */

@@ -334,11 +334,12 @@ class CoreSG:
         self.ctx.check(lib().cs_sweep_timing(self.h, C.byref(gm), C.byref(km)))
         return float(gm.value), float(km.value)
 
-    def set_sweep_shape(self, group=0, block=0):
-        self.ctx.check(lib().cs_set_sweep_shape(self.h, group, block))
+    def set_sweep_shape(self, flatten=0, block=0):
+        """flatten: divisor of the flatten rule (0 auto, 0xFFFFFFFF never); block threads."""
+        self.ctx.check(lib().cs_set_sweep_shape(self.h, flatten, block))
 
     def autotune(self, mpts_values):
         mp = np.ascontiguousarray(mpts_values, np.uint32)
-        g, b = C.c_uint32(), C.c_uint32()
-        self.ctx.check(lib().cs_autotune_sweep(self.h, _ptr(mp), len(mp), C.byref(g), C.byref(b)))
-        return int(g.value), int(b.value)
+        f, b = C.c_uint32(), C.c_uint32()
+        self.ctx.check(lib().cs_autotune_sweep(self.h, _ptr(mp), len(mp), C.byref(f), C.byref(b)))
+        return int(f.value), int(b.value)

@@ -115,14 +115,18 @@ struct Graph {
     // Hubness selection of the last cs_select_bridges.
     std::vector<uint32_t> selected;
 
-    // Batched sweep state (mst.cu).
+    // Batched sweep state (sweep.cu): a chain of plans, one per pass of <= 32 MSTs.
     SweepPlan* plan = nullptr;
-    uint32_t sweep_group = 0, sweep_block = 0;  // 0 = autotuned/cached
+    uint32_t sweep_K = 0;                      // MSTs of the last sweep
+    uint32_t sweep_block = 0;                  // 0 = autotuned/cached
+    uint32_t sweep_flatten = 0xFFFFFFFEu;      // kFlattenAuto, or a divisor (0: never)
 
     ~Graph();
     void invalidate_edges() { edges_valid = false; }
     void ensure_capacity(uint64_t need, bool keep);
 };
+
+constexpr uint32_t kFlattenAuto = 0xFFFFFFFEu;
 
 // ---- module entry points (implemented in the .cu files) ----------------------------
 
@@ -133,7 +137,7 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
                                  DevBuf& tmp_off);
 void launch_core(const Graph& g, uint32_t mpts, float* core, cudaStream_t s);
 
-// mst.cu
+// mst.cu, sweep.cu
 struct MstHost {
     uint64_t nedges = 0;
     uint32_t ncomp = 0;
@@ -148,6 +152,8 @@ double exact_sum_from_bins(const uint64_t* bins256);
 /// whose roots are their sets' smallest nodes; component counts -> ncomp[K].
 void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_t* lab_all, uint32_t* bc,
                    unsigned long long* ncomp);
+/// In-place exclusive scan of K rows of nt u32 tile counts; row totals -> totals[K].
+void launch_scan_tiles(Ctx& c, uint32_t* tiles, uint32_t nt, uint32_t K, unsigned long long* totals);
 
 // knn.cu
 void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,

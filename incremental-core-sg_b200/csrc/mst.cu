@@ -21,11 +21,9 @@
 //
 // Plain path (cs_extract): edges(mpts) materialised per call exactly as
 // CoreSG::edges does, then one kernel per phase with a host read of the counters
-// after every phase A (the reference's round loop, moved to the device).
-// Batched path (cs_extract_sweep): the cached base edge list is reweighted on the
-// fly for every mpts; all K MSTs run inside ONE cooperative persistent kernel,
-// G MSTs at a time (their union-find state stays L2-resident), with a bounded grid
-// barrier between phases; the whole sequence is captured once in a CUDA graph.
+// after every phase A (the reference's round loop, moved to the device).  The
+// batched sweep (cs_extract_sweep) is in sweep.cu; it shares the labelling and
+// exact-sum helpers defined here.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -56,7 +54,6 @@ namespace {
 constexpr int kMaxRounds = 64;
 constexpr int kThreads = 256;
 constexpr int kTileWords = 2048;  // compaction tile: 256 threads x 8 words
-constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 
 inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     uint64_t b = (work + threads - 1) / threads;
@@ -170,139 +167,6 @@ __global__ void k_phase_b(MstView m, const uint32_t* __restrict__ eu, const uint
         root_step(m, m.touched[t], eu, ev, sbins, status);
     }
     flush_bins(sbins, m.bins);
-}
-
-// ---- the batched persistent kernel ------------------------------------------------------
-
-struct SweepArgs {
-    uint32_t n, E, K, G, W;
-    const uint32_t* eu;
-    const uint32_t* ev;
-    const float* ew;
-    const float* core;          // K*n
-    uint32_t* parent;           // K*n
-    unsigned long long* best;   // G*n
-    uint32_t* touched;          // G*n
-    uint32_t* wl;               // G*2*E
-    uint32_t* bitmap;           // K*W
-    unsigned long long* bins;   // K*256
-    uint32_t* ctr;              // G*8
-    unsigned* bar;              // [0] count, [1] generation
-    int* status;
-    uint64_t limit_ns;
-};
-
-__device__ __forceinline__ MstView view_of(const SweepArgs& a, uint32_t slot, uint32_t j) {
-    MstView m;
-    m.parent = a.parent + static_cast<uint64_t>(j) * a.n;
-    m.best = a.best + static_cast<uint64_t>(slot) * a.n;
-    m.touched = a.touched + static_cast<uint64_t>(slot) * a.n;
-    m.wl0 = a.wl + static_cast<uint64_t>(slot) * 2 * a.E;
-    m.wl1 = m.wl0 + a.E;
-    m.bitmap = a.bitmap + static_cast<uint64_t>(j) * a.W;
-    m.bins = a.bins + static_cast<uint64_t>(j) * 256;
-    m.ctr = a.ctr + slot * 8;
-    m.core = a.core + static_cast<uint64_t>(j) * a.n;
-    return m;
-}
-
-__global__ void __launch_bounds__(512) k_sweep(SweepArgs a) {
-    __shared__ unsigned long long sbins[256];
-    for (int b = threadIdx.x; b < 256; b += blockDim.x) sbins[b] = 0;
-    const uint64_t gtid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint64_t gstride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-
-    for (uint32_t g0 = 0; g0 < a.K; g0 += a.G) {
-        const uint32_t slots = min(a.G, a.K - g0);
-        // -- group init: identity parents, zero counters (best[] is all-empty
-        //    between groups: every touched root is reset in its phase B).
-        const uint64_t pn = static_cast<uint64_t>(slots) * a.n;
-        for (uint64_t t = gtid; t < pn; t += gstride) {
-            a.parent[static_cast<uint64_t>(g0) * a.n + t] = static_cast<uint32_t>(t % a.n);
-        }
-        if (blockIdx.x == 0 && threadIdx.x < slots * 8) a.ctr[threadIdx.x] = 0;
-        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-
-        uint32_t active = (slots >= 32) ? 0xFFFFFFFFu : ((1u << slots) - 1u);
-        int r = 0;
-        for (; r < kMaxRounds; ++r) {
-            // ---- phase A
-            if (r <= 1) {
-                const uint64_t padded = (static_cast<uint64_t>(a.E) + 31) & ~31ull;
-                for (uint64_t t = gtid; t < padded; t += gstride) {
-                    const bool valid = t < a.E;
-                    uint32_t u = 0, v = 0;
-                    float w = 0.0f;
-                    if (valid) {
-                        u = __ldg(a.eu + t);
-                        v = __ldg(a.ev + t);
-                        w = __ldg(a.ew + t);
-                    }
-                    for (uint32_t s = 0; s < slots; ++s) {
-                        if (!(active >> s & 1u)) continue;
-                        edge_step<true>(view_of(a, s, g0 + s), static_cast<uint32_t>(t), valid, u, v, w,
-                                        a.n, r, r == 1);
-                    }
-                }
-            } else {
-                for (uint32_t s = 0; s < slots; ++s) {
-                    if (!(active >> s & 1u)) continue;
-                    const MstView m = view_of(a, s, g0 + s);
-                    const uint32_t cnt = __ldcg(m.ctr + (r & 1));
-                    const uint32_t* in = (r & 1) ? m.wl1 : m.wl0;
-                    const uint64_t padded = (static_cast<uint64_t>(cnt) + 31) & ~31ull;
-                    for (uint64_t t = gtid; t < padded; t += gstride) {
-                        const bool valid = t < cnt;
-                        uint32_t i = 0, u = 0, v = 0;
-                        float w = 0.0f;
-                        if (valid) {
-                            i = __ldcg(in + t);
-                            u = __ldg(a.eu + i);
-                            v = __ldg(a.ev + i);
-                            w = __ldg(a.ew + i);
-                        }
-                        edge_step<true>(m, i, valid, u, v, w, a.n, r, true);
-                    }
-                }
-            }
-            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-
-            // ---- termination: an MST with no live edge left is done
-            for (uint32_t s = 0; s < slots; ++s) {
-                if (!(active >> s & 1u)) continue;
-                if (__ldcg(a.ctr + s * 8 + 2 + (r & 1)) == 0) active &= ~(1u << s);
-            }
-            if (active == 0) break;
-
-            // ---- phase B
-            for (uint32_t s = 0; s < slots; ++s) {
-                if (!(active >> s & 1u)) continue;
-                const MstView m = view_of(a, s, g0 + s);
-                const uint32_t tcnt = __ldcg(m.ctr + 2 + (r & 1));
-                for (uint64_t t = gtid; t < tcnt; t += gstride) {
-                    root_step(m, __ldcg(m.touched + t), a.eu, a.ev, sbins, a.status);
-                }
-                flush_bins(sbins, m.bins);
-            }
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
-                for (uint32_t s = 0; s < slots; ++s) {
-                    a.ctr[s * 8 + (r & 1)] = 0;            // next round's append target
-                    a.ctr[s * 8 + 2 + ((r + 1) & 1)] = 0;  // next round's touched count
-                }
-            }
-            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-        }
-        if (r == kMaxRounds && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusRoundLimit);
-    }
-}
-
-/// Core tables of K mpts values: core[j][v], one dist row read per node.
-__global__ void k_core_multi(const float* __restrict__ dists, const uint32_t* __restrict__ counts,
-                             uint32_t n, uint32_t k, const uint32_t* __restrict__ mpts, uint32_t K,
-                             float* __restrict__ core) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    for (uint32_t j = 0; j < K; ++j) core[static_cast<uint64_t>(j) * n + v] = core_of(dists, counts, k, v, mpts[j]);
 }
 
 // ---- labels: dense, numbered by smallest node -------------------------------------------
@@ -530,6 +394,11 @@ void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_
     count_launch(c, 4);
 }
 
+void launch_scan_tiles(Ctx& c, uint32_t* tiles, uint32_t nt, uint32_t K, unsigned long long* totals) {
+    k_scan_tiles<<<K, 1024, 0, c.stream>>>(tiles, nt, totals);
+    count_launch(c);
+}
+
 namespace {
 
 void launch_compact(Ctx& c, const uint32_t* bitmap, uint32_t W, uint32_t K, uint32_t* tiles,
@@ -651,300 +520,6 @@ void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_la
     if (out_labels && n) copy_d2h(c, out_labels, lab.p, static_cast<uint64_t>(n) * 4);
 }
 
-// ============================================================================
-// batched sweep
-// ============================================================================
-
-struct SweepPlan {
-    uint32_t n = 0, E = 0, K = 0, G = 0, W = 0, block = 0, grid = 0;
-    bool labels = false;
-    uint64_t edges_version = 0;
-    DevBuf mpts, core, parent, best, touched, wl, bitmap, bins, ctr, bar, status, tiles, lab, out, counts;
-    uint32_t nbl = 0, ntl = 0;
-    cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
-    bool captured = false;
-    std::vector<uint32_t> host_mpts;
-    const void* key_ptrs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;  // around the persistent kernel
-    float last_graph_ms = 0.0f, last_kernel_ms = 0.0f;
-    ~SweepPlan() {
-        if (exec_pre) cudaGraphExecDestroy(exec_pre);
-        if (exec_main) cudaGraphExecDestroy(exec_main);
-        if (exec_post) cudaGraphExecDestroy(exec_post);
-        if (ev_k0) cudaEventDestroy(ev_k0);
-        if (ev_k1) cudaEventDestroy(ev_k1);
-    }
-};
-
-void sweep_free(SweepPlan* p) { delete p; }
-
-namespace {
-
-std::mutex g_tune_mu;
-std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, std::pair<uint32_t, uint32_t>> g_tuned;
-
-SweepArgs args_of(Graph& g, SweepPlan& p) {
-    SweepArgs a;
-    a.n = p.n;
-    a.E = p.E;
-    a.K = p.K;
-    a.G = p.G;
-    a.W = p.W;
-    a.eu = g.eu.as<uint32_t>();
-    a.ev = g.ev.as<uint32_t>();
-    a.ew = g.ew.as<float>();
-    a.core = p.core.as<float>();
-    a.parent = p.parent.as<uint32_t>();
-    a.best = p.best.as<unsigned long long>();
-    a.touched = p.touched.as<uint32_t>();
-    a.wl = p.wl.as<uint32_t>();
-    a.bitmap = p.bitmap.as<uint32_t>();
-    a.bins = p.bins.as<unsigned long long>();
-    a.ctr = p.ctr.as<uint32_t>();
-    a.bar = p.bar.as<unsigned>();
-    a.status = p.status.as<int>();
-    a.limit_ns = kBarrierLimitNs;
-    return a;
-}
-
-/// The sweep is enqueued in three parts, each captured into its own CUDA graph:
-///   pre   reset the per-sweep state, core tables of the K mpts values
-///   main  the persistent cooperative Boruvka kernel (all K MSTs)
-///   post  labels and tree compaction
-/// so stream events between the parts time the persistent kernel alone.
-void enqueue_pre(Graph& g, SweepPlan& p) {
-    Ctx& c = *g.ctx;
-    const uint64_t n = p.n;
-    CSB_CUDA(cudaMemsetAsync(p.status.p, 0, 64, c.stream));
-    CSB_CUDA(cudaMemsetAsync(p.bar.p, 0, 64, c.stream));
-    CSB_CUDA(cudaMemsetAsync(p.bitmap.p, 0, static_cast<uint64_t>(p.K) * p.W * 4, c.stream));
-    CSB_CUDA(cudaMemsetAsync(p.bins.p, 0, static_cast<uint64_t>(p.K) * 256 * 8, c.stream));
-    CSB_CUDA(cudaMemsetAsync(p.best.p, 0xFF, static_cast<uint64_t>(p.G) * std::max<uint64_t>(n, 1) * 8, c.stream));
-    if (n) {
-        k_core_multi<<<blocks_for(n), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(),
-                                                              p.n, g.k, p.mpts.as<uint32_t>(), p.K,
-                                                              p.core.as<float>());
-        count_launch(c);
-    }
-}
-
-void enqueue_main(Graph& g, SweepPlan& p) {
-    Ctx& c = *g.ctx;
-    if (!p.n) return;
-    SweepArgs a = args_of(g, p);
-    void* params[] = {&a};
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(p.grid);
-    cfg.blockDim = dim3(p.block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
-    count_launch(c);
-}
-
-void enqueue_post(Graph& g, SweepPlan& p) {
-    Ctx& c = *g.ctx;
-    const uint64_t n = p.n;
-    if (!n) return;
-    if (p.labels) {
-        launch_labels(c, p.parent.as<uint32_t>(), p.n, p.K, p.lab.as<uint32_t>(), p.tiles.as<uint32_t>(),
-                      p.counts.as<unsigned long long>());
-    }
-    launch_compact(c, p.bitmap.as<uint32_t>(), p.W, p.K, p.tiles.as<uint32_t>() + static_cast<uint64_t>(p.K) * p.nbl,
-                   p.counts.as<unsigned long long>() + p.K, g.eu.as<uint32_t>(), g.ev.as<uint32_t>(), g.ew.as<float>(),
-                   p.core.as<float>(), p.n, n - 1, p.out.as<cs_edge>(), p.status.as<int>());
-}
-
-using Enqueue = void (*)(Graph&, SweepPlan&);
-
-/// Capture one part into a graph; false (and no graph) when capture is refused.
-bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
-    Ctx& c = *g.ctx;
-    *out = nullptr;
-    if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    const uint64_t before = c.launches;
-    bool ok = true;
-    try {
-        f(g, p);
-    } catch (...) {
-        ok = false;
-    }
-    c.launches = before;  // counted when replayed
-    cudaGraph_t graph = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
-    ok = ok && e == cudaSuccess && graph;
-    if (ok) ok = cudaGraphInstantiate(out, graph, 0) == cudaSuccess;
-    if (graph) cudaGraphDestroy(graph);
-    if (!ok) {
-        cudaGetLastError();
-        *out = nullptr;
-    }
-    return ok;
-}
-
-SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t G, uint32_t block, bool labels) {
-    Ctx& c = *g.ctx;
-    graph_build_edges(g);
-    SweepPlan* p = new SweepPlan();
-    try {
-        p->n = static_cast<uint32_t>(g.n);
-        p->E = static_cast<uint32_t>(g.e_total);
-        p->key_ptrs[0] = g.eu.p;
-        p->key_ptrs[1] = g.ev.p;
-        p->key_ptrs[2] = g.ew.p;
-        p->key_ptrs[3] = g.dists.p;
-        p->key_ptrs[4] = g.counts.p;
-        CSB_CUDA(cudaEventCreate(&p->ev_k0));
-        CSB_CUDA(cudaEventCreate(&p->ev_k1));
-        p->K = K;
-        p->G = std::max<uint32_t>(1, std::min<uint32_t>(G, std::min<uint32_t>(K, 32)));
-        p->W = (p->E + 31) / 32 + 1;
-        p->block = block;
-        p->labels = labels;
-        const uint64_t n = std::max<uint32_t>(p->n, 1);
-        const uint64_t E = std::max<uint32_t>(p->E, 1);
-        p->mpts.ensure(K * 4 + 4);
-        p->core.ensure(K * n * 4);
-        p->parent.ensure(K * n * 4);
-        p->best.ensure(p->G * n * 8);
-        p->touched.ensure(p->G * n * 4);
-        p->wl.ensure(p->G * 2 * E * 4);
-        p->bitmap.ensure(static_cast<uint64_t>(K) * p->W * 4);
-        p->bins.ensure(static_cast<uint64_t>(K) * 256 * 8);
-        p->ctr.ensure(static_cast<uint64_t>(p->G) * 8 * 4 + 64);
-        p->bar.ensure(64);
-        p->status.ensure(64);
-        p->nbl = blocks_for(n);
-        p->ntl = std::max<uint32_t>(1, (p->W + kTileWords - 1) / kTileWords);
-        p->tiles.ensure(static_cast<uint64_t>(K) * (p->nbl + p->ntl) * 4 + 64);
-        if (labels) p->lab.ensure(K * n * 4);
-        p->out.ensure(K * std::max<uint64_t>(n - 1, 1) * sizeof(cs_edge));
-        p->counts.ensure(static_cast<uint64_t>(2 * K) * 8 + 64);
-        int occ = 0;
-        CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep, static_cast<int>(block), 0));
-        if (occ < 1) fail(CS_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
-        p->grid = static_cast<uint32_t>(c.sm_count) * static_cast<uint32_t>(occ);
-        // capture the three parts into CUDA graphs (replayed by run_plan)
-        bool ok = capture_part(g, *p, enqueue_pre, &p->exec_pre);
-        ok = capture_part(g, *p, enqueue_main, &p->exec_main) && ok;
-        ok = capture_part(g, *p, enqueue_post, &p->exec_post) && ok;
-        p->captured = ok;
-    } catch (...) {
-        delete p;
-        throw;
-    }
-    return p;
-}
-
-uint64_t kernels_pre(const SweepPlan& p) { return p.n ? 1 : 0; }
-uint64_t kernels_post(const SweepPlan& p) { return p.n ? ((p.labels ? 4 : 0) + 3) : 0; }
-
-void run_plan(Graph& g, SweepPlan& p, float* out_ms) {
-    Ctx& c = *g.ctx;
-    cudaEvent_t e0, e1;
-    CSB_CUDA(cudaEventCreate(&e0));
-    CSB_CUDA(cudaEventCreate(&e1));
-    CSB_CUDA(cudaMemcpyAsync(p.mpts.p, p.host_mpts.data(), p.K * 4, cudaMemcpyHostToDevice, c.stream));
-    CSB_CUDA(cudaEventRecord(e0, c.stream));
-    if (p.exec_pre) {
-        CSB_CUDA(cudaGraphLaunch(p.exec_pre, c.stream));
-        count_launch(c, kernels_pre(p));
-    } else {
-        enqueue_pre(g, p);
-    }
-    CSB_CUDA(cudaEventRecord(p.ev_k0, c.stream));
-    if (p.exec_main) {
-        CSB_CUDA(cudaGraphLaunch(p.exec_main, c.stream));
-        count_launch(c, p.n ? 1 : 0);
-    } else {
-        enqueue_main(g, p);
-    }
-    CSB_CUDA(cudaEventRecord(p.ev_k1, c.stream));
-    if (p.exec_post) {
-        CSB_CUDA(cudaGraphLaunch(p.exec_post, c.stream));
-        count_launch(c, kernels_post(p));
-    } else {
-        enqueue_post(g, p);
-    }
-    CSB_CUDA(cudaEventRecord(e1, c.stream));
-    CSB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.0f, kms = 0.0f;
-    CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    CSB_CUDA(cudaEventElapsedTime(&kms, p.ev_k0, p.ev_k1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    p.last_graph_ms = ms;
-    p.last_kernel_ms = kms;
-    if (out_ms) *out_ms = ms;
-    status_check(c, p.status.as<int>());
-}
-
-}  // namespace
-
-void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms) {
-    if (K == 0) fail(CS_ERR_INVALID, "sweep: K must be positive");
-    for (uint32_t j = 0; j < K; ++j) {
-        if (mpts[j] > g.k) fail(CS_ERR_INVALID, "sweep: mpts exceeds k_max");
-    }
-    graph_build_edges(g);
-    Ctx& c = *g.ctx;
-    uint32_t G = g.sweep_group, B = g.sweep_block;
-    if (!G || !B) {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tuned.find(std::make_tuple(static_cast<uint32_t>(g.n), static_cast<uint32_t>(g.e_total), K, c.sm_count));
-        if (it != g_tuned.end()) {
-            if (!G) G = it->second.first;
-            if (!B) B = it->second.second;
-        }
-    }
-    if (!G) G = std::min<uint32_t>(K, 4);
-    if (!B) B = 256;
-    SweepPlan* p = g.plan;
-    const bool reuse = p && p->n == g.n && p->E == g.e_total && p->K == K &&
-                       p->G == std::max<uint32_t>(1, std::min(G, std::min<uint32_t>(K, 32))) && p->block == B &&
-                       p->labels == want_labels && p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
-                       p->key_ptrs[2] == g.ew.p && p->key_ptrs[3] == g.dists.p && p->key_ptrs[4] == g.counts.p;
-    if (!reuse) {
-        if (g.plan) sweep_free(g.plan);
-        g.plan = nullptr;
-        g.plan = make_plan(g, K, G, B, want_labels);
-        p = g.plan;
-    }
-    p->host_mpts.assign(mpts, mpts + K);
-    for (auto& m : p->host_mpts) {
-        if (m == 0) m = 1;  // CoreSG::edges treats mpts 0 as 1
-    }
-    run_plan(g, *p, out_ms);
-}
-
-void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res) {
-    SweepPlan* p = g.plan;
-    if (!p) fail(CS_ERR_STATE, "sweep_fetch: no sweep has run");
-    if (index >= p->K) fail(CS_ERR_INVALID, "sweep_fetch: index out of range");
-    if (out_labels && !p->labels) fail(CS_ERR_STATE, "sweep_fetch: the sweep ran without labels");
-    Ctx& c = *g.ctx;
-    unsigned long long ne = 0;
-    uint64_t bins[256];
-    CSB_CUDA(cudaMemcpyAsync(&ne, p->counts.as<unsigned long long>() + p->K + index, 8, cudaMemcpyDeviceToHost, c.stream));
-    CSB_CUDA(cudaMemcpyAsync(bins, p->bins.as<unsigned long long>() + static_cast<uint64_t>(index) * 256,
-                             sizeof(bins), cudaMemcpyDeviceToHost, c.stream));
-    CSB_CUDA(cudaStreamSynchronize(c.stream));
-    res->nedges = ne;
-    res->ncomp = static_cast<uint32_t>(p->n - ne);
-    res->weight = exact_sum_from_bins(bins);
-    const uint64_t cap = p->n ? p->n - 1 : 0;
-    if (out_edges && ne) copy_d2h(c, out_edges, p->out.as<cs_edge>() + index * cap, ne * sizeof(cs_edge));
-    if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(index) * p->n, static_cast<uint64_t>(p->n) * 4);
-}
-
 }  // namespace csb
 
 // ============================================================================
@@ -964,105 +539,6 @@ cs_status cs_extract(cs_graph* gp, uint32_t mpts, cs_edge* out_edges, uint32_t* 
         if (out_nedges) *out_nedges = r.nedges;
         if (out_ncomp) *out_ncomp = r.ncomp;
         if (out_weight) *out_weight = r.weight;
-    });
-}
-
-cs_status cs_extract_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
-                           uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
-                           double* out_weight) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep: null mpts");
-        sweep_run(*g, mpts, K, out_labels != nullptr, nullptr);
-        const uint64_t cap = g->n ? g->n - 1 : 0;
-        for (uint32_t j = 0; j < K; ++j) {
-            MstHost r;
-            sweep_fetch(*g, j, out_edges ? out_edges + j * cap : nullptr,
-                        out_labels ? out_labels + static_cast<uint64_t>(j) * g->n : nullptr, &r);
-            if (out_nedges) out_nedges[j] = r.nedges;
-            if (out_ncomp) out_ncomp[j] = r.ncomp;
-            if (out_weight) out_weight[j] = r.weight;
-        }
-    });
-}
-
-cs_status cs_extract_sweep_device(cs_graph* gp, const uint32_t* mpts, uint32_t K, float* out_ms) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep_device: null mpts");
-        sweep_run(*g, mpts, K, true, out_ms);
-    });
-}
-
-cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
-                         uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        MstHost r;
-        sweep_fetch(*g, index, out_edges, out_labels, &r);
-        if (out_nedges) *out_nedges = r.nedges;
-        if (out_ncomp) *out_ncomp = r.ncomp;
-        if (out_weight) *out_weight = r.weight;
-    });
-}
-
-cs_status cs_sweep_timing(cs_graph* gp, float* graph_ms, float* kernel_ms) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        if (!g->plan) fail(CS_ERR_STATE, "cs_sweep_timing: no sweep has run");
-        if (graph_ms) *graph_ms = g->plan->last_graph_ms;
-        if (kernel_ms) *kernel_ms = g->plan->last_kernel_ms;
-    });
-}
-
-cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t group, uint32_t block_threads) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        CSB_REQUIRE(block_threads == 0 || block_threads == 128 || block_threads == 256 || block_threads == 512,
-                    "cs_set_sweep_shape: block must be 128, 256 or 512");
-        CSB_REQUIRE(group <= 32, "cs_set_sweep_shape: group must be <= 32");
-        g->sweep_group = group;
-        g->sweep_block = block_threads;
-    });
-}
-
-cs_status cs_autotune_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, uint32_t* out_group,
-                            uint32_t* out_block) {
-    Graph* g = reinterpret_cast<Graph*>(gp);
-    return guarded(g ? g->ctx : nullptr, [&] {
-        CSB_REQUIRE(mpts != nullptr && K > 0, "cs_autotune_sweep: empty mpts");
-        const uint32_t saved_g = g->sweep_group, saved_b = g->sweep_block;
-        float best_ms = 1e30f;
-        uint32_t best_g = 0, best_b = 0;
-        const uint32_t groups[] = {1, 2, 4, 8, 16, 32};
-        const uint32_t blocks[] = {256, 512};
-        for (uint32_t G : groups) {
-            if (G > K && G != 1) continue;
-            for (uint32_t B : blocks) {
-                g->sweep_group = G;
-                g->sweep_block = B;
-                float ms = 0.0f, tot = 0.0f;
-                sweep_run(*g, mpts, K, true, &ms);  // build + warm
-                for (int rep = 0; rep < 2; ++rep) {
-                    sweep_run(*g, mpts, K, true, &ms);
-                    tot += ms;
-                }
-                if (tot < best_ms) {
-                    best_ms = tot;
-                    best_g = G;
-                    best_b = B;
-                }
-            }
-        }
-        g->sweep_group = saved_g;
-        g->sweep_block = saved_b;
-        {
-            std::lock_guard<std::mutex> lk(g_tune_mu);
-            g_tuned[std::make_tuple(static_cast<uint32_t>(g->n), static_cast<uint32_t>(g->e_total), K, g->ctx->sm_count)] =
-                std::make_pair(best_g, best_b);
-        }
-        if (out_group) *out_group = best_g;
-        if (out_block) *out_block = best_b;
     });
 }
 

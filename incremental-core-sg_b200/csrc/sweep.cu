@@ -1,0 +1,898 @@
+// The batched mpts sweep: up to 32 MSTs of one CORE-SG in one persistent launch.
+//
+// CoreSG::all_msts (src/coresg.cpp:412-417) runs K independent extractions, each
+// rebuilding edges(mpts) and a Boruvka (src/mst.cpp:79-151).  Here the K MSTs of a
+// pass share everything that can be shared:
+//
+//   * the edge list is built once per CORE-SG (graph.cu) and reweighted on the fly,
+//     w'_j = max(w, core_j(u), core_j(v)), with core_j read from the k-NN distance
+//     row of the node (one 128-byte row holds every core distance of a node);
+//   * one warp handles one edge (or one node's emitted segment) for all MSTs at once:
+//     lane j is MST j.  Per-node state is node-major -- parent[v][32], best[v][32] --
+//     so a node's state for all 32 MSTs is one 128/256-byte line and every per-node
+//     access of the warp is coalesced;
+//   * membership of edge i in the 32 trees is one bit-packed word tree[i]; liveness
+//     likewise (live[i]); a single worklist of edges still live in any MST serves all
+//     of them;
+//   * rounds 0 and 1 walk each node's emitted segment (the node-major enumeration of
+//     src/knn_graph.cpp:132-200), so the emitter-side atomicMin of every lane is
+//     aggregated over the segment in registers and issued once;
+//   * between rounds the union-find forests are flattened (parent[v][j] = root), so
+//     the next round's root lookups are single coalesced loads;
+//   * worklist and touched-root appends are buffered per warp in shared memory and
+//     flushed 32 at a time (one atomicAdd per flush);
+//   * the phases are separated by a bounded grid barrier of a cooperative launch, and
+//     the state reset, the persistent kernel and the finishing kernels (labels, tree
+//     compaction, exact weights) are each captured once into a CUDA graph.
+//
+// Per round r, lane j (MST j):
+//   A  every live edge finds the roots of its endpoints; if they differ it offers the
+//      key (w'_j bits << 32 | i) to best[root][j] of both with atomicMin; the first
+//      offer to a root in a round records the root in the touched list;
+//   B  every touched root takes best[root][j]; the first lane to set bit j of tree[i]
+//      unites the endpoints (roots linked larger-under-smaller) and resets best.
+// The result is the unique minimum spanning forest of each mpts under (weight bits,
+// edge index), i.e. the reference Boruvka's tree (pack_edge, src/mst.cpp:19-24).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "common.cuh"
+#include "engine.hpp"
+
+namespace csb {
+namespace {
+
+constexpr int kLanes = 32;
+constexpr int kMaxRounds = 64;
+constexpr int kThreads = 256;
+constexpr uint64_t kBarrierLimitNs = 2000000000ull;
+constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
+constexpr int kMaxBlock = 512;
+
+inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
+    uint64_t b = (work + threads - 1) / threads;
+    return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(b, 1u << 30)));
+}
+
+struct SweepArgs {
+    uint32_t n, E, e_knn, K, k;
+    uint32_t flatten_div;  // flatten when the next worklist exceeds n / flatten_div (0: never)
+    const uint32_t* eu;
+    const uint32_t* ev;
+    const float* ew;
+    const uint32_t* node_off;  // [n+1] emitted-segment offsets
+    const float* dists;        // [n][k]
+    const uint32_t* counts;    // [n]
+    const uint32_t* mpts;      // [K]
+    uint32_t* parent;          // [n][32]
+    unsigned long long* best;  // [n][32]
+    uint32_t* tree;            // [E] bit j: edge in MST j
+    uint32_t* live;            // [E] bit j: edge live in MST j
+    uint32_t* wl;              // [2][E]
+    uint32_t* tlist;           // [n]
+    uint32_t* tflag;           // [n]
+    uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] touched counts; [4] rounds
+    unsigned* bar;
+    int* status;
+    uint64_t limit_ns;
+};
+
+__device__ __forceinline__ float core_lane(const SweepArgs& a, uint32_t x, uint32_t m) {
+    const uint32_t c = __ldg(a.counts + x);
+    if (c == 0) return __int_as_float(0x7f800000);
+    const uint32_t pos = (m < c ? m : c) - 1;  // m >= 1
+    return __ldg(a.dists + static_cast<uint64_t>(x) * a.k + pos);
+}
+
+/// find with path halving on forest j of the node-major parent array.
+__device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_t j) {
+    for (;;) {
+        const uint32_t p = __ldcg(parent + static_cast<uint64_t>(x) * kLanes + j);
+        if (p == x) return x;
+        const uint32_t gp = __ldcg(parent + static_cast<uint64_t>(p) * kLanes + j);
+        if (gp == p) return p;
+        parent[static_cast<uint64_t>(x) * kLanes + j] = gp;
+        x = gp;
+    }
+}
+
+__device__ __forceinline__ bool unite32(uint32_t* parent, uint32_t a, uint32_t b, uint32_t j, int* status) {
+    for (int it = 0; it < (1 << 20); ++it) {
+        a = find32(parent, a, j);
+        b = find32(parent, b, j);
+        if (a == b) return false;
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(parent + static_cast<uint64_t>(b) * kLanes + j, b, a) == b) return true;
+    }
+    atomicOr(status, kStatusUnionLimit);
+    return false;
+}
+
+/// Per-warp list buffer in shared memory: appends are staged and flushed to the
+/// global list 32 at a time with one atomicAdd on the list's counter.
+struct WarpList {
+    uint32_t* stage;  // 32 entries of this warp's shared memory
+    uint32_t* list;
+    uint32_t* counter;
+    uint32_t n;  // warp-uniform fill
+    __device__ __forceinline__ void flush() {
+        if (n == 0) return;
+        __syncwarp();
+        const unsigned lane = threadIdx.x & 31u;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(counter, n);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (lane < n) list[base + lane] = stage[lane];
+        __syncwarp();
+        n = 0;
+    }
+    /// warp-collective: every lane with `pred` appends `v`
+    __device__ __forceinline__ void push(bool pred, uint32_t v) {
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, pred);
+        if (!m) return;
+        const uint32_t c = __popc(m);
+        if (n + c > 32) flush();
+        const unsigned lane = threadIdx.x & 31u;
+        if (pred) stage[n + __popc(m & ((1u << lane) - 1u))] = v;
+        __syncwarp();
+        n += c;
+    }
+};
+
+/// Record roots offered to for the first time this round (warp-collective).
+__device__ __forceinline__ void touch(const SweepArgs& a, bool t, uint32_t root, WarpList& tl) {
+    const unsigned tm = __ballot_sync(0xFFFFFFFFu, t);
+    if (!tm) return;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, t ? root : kInvalid) & tm;
+    bool first = false;
+    if (t && static_cast<int>(lane) == __ffs(grp) - 1) first = atomicOr(a.tflag + root, grp) == 0u;
+    tl.push(first, root);
+}
+
+/// Phase A for one edge whose live lanes are `lm` (warp-collective).
+__device__ __forceinline__ void edge_lanes(const SweepArgs& a, uint32_t i, uint32_t lm, int r, bool flat,
+                                           uint32_t mj, WarpList& tl, WarpList& wlo) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t u = __ldg(a.eu + i), v = __ldg(a.ev + i);
+    const float w = __ldg(a.ew + i);
+    const bool act = (lm >> lane) & 1u;
+    bool live = false, tu = false, tv = false;
+    uint32_t ru = u, rv = v;
+    if (act && u < a.n && v < a.n) {
+        const float wp = max_ref(w, max_ref(core_lane(a, u, mj), core_lane(a, v, mj)));
+        if (r > 0) {
+            ru = flat ? __ldcg(a.parent + static_cast<uint64_t>(u) * kLanes + lane) : find32(a.parent, u, lane);
+            rv = flat ? __ldcg(a.parent + static_cast<uint64_t>(v) * kLanes + lane) : find32(a.parent, v, lane);
+        }
+        live = ru != rv;
+        if (live) {
+            const unsigned long long key = pack_key(wp, i);
+            tu = atomicMin(a.best + static_cast<uint64_t>(ru) * kLanes + lane, key) == kNoKey;
+            tv = atomicMin(a.best + static_cast<uint64_t>(rv) * kLanes + lane, key) == kNoKey;
+        }
+    }
+    touch(a, tu, ru, tl);
+    touch(a, tv, rv, tl);
+    if (r >= 1) {
+        const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
+        if (L && lane == 0) a.live[i] = L;
+        wlo.push(L != 0 && lane == 0, i);
+    }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
+    __shared__ uint32_t s_stage[kMaxBlock / 32][2][32];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned wib = threadIdx.x >> 5;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const bool act = lane < a.K;
+    const uint32_t mj = act ? __ldg(a.mpts + lane) : 1u;
+    const uint32_t allmask = a.K >= 32 ? 0xFFFFFFFFu : ((1u << a.K) - 1u);
+    bool flat = true;  // parents are the identity at the start
+    int r = 0;
+    for (; r < kMaxRounds; ++r) {
+        const int par = r & 1;
+        WarpList tl{s_stage[wib][0], a.tlist, a.ctr + 2 + par, 0};
+        WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>((r + 1) & 1) * a.E, a.ctr + ((r + 1) & 1), 0};
+        // ---- phase A
+        if (r <= 1) {
+            // k-NN edges, node by node: the emitter's roots and core distances are
+            // loaded once, its offers are reduced in registers over its segment
+            for (uint32_t p = gw; p < a.n; p += nw) {
+                const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
+                if (beg == end) continue;
+                const float cp = act ? core_lane(a, p, mj) : 0.0f;
+                uint32_t rp = p;
+                if (r > 0 && act) rp = flat ? __ldcg(a.parent + static_cast<uint64_t>(p) * kLanes + lane) : find32(a.parent, p, lane);
+                unsigned long long seg = kNoKey;
+                for (uint32_t i = beg; i < end; ++i) {
+                    const uint32_t eu = __ldg(a.eu + i), ev = __ldg(a.ev + i);
+                    const float w = __ldg(a.ew + i);
+                    const uint32_t q = eu == p ? ev : eu;
+                    bool live = false, tq = false;
+                    uint32_t rq = q;
+                    if (act) {
+                        const float wp = max_ref(w, max_ref(cp, core_lane(a, q, mj)));
+                        if (r > 0) rq = flat ? __ldcg(a.parent + static_cast<uint64_t>(q) * kLanes + lane) : find32(a.parent, q, lane);
+                        live = rp != rq;
+                        if (live) {
+                            const unsigned long long key = pack_key(wp, i);
+                            seg = key < seg ? key : seg;
+                            tq = atomicMin(a.best + static_cast<uint64_t>(rq) * kLanes + lane, key) == kNoKey;
+                        }
+                    }
+                    touch(a, tq, rq, tl);
+                    if (r == 1) {
+                        const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
+                        if (L && lane == 0) a.live[i] = L;
+                        wlo.push(L != 0 && lane == 0, i);
+                    }
+                }
+                bool tp = false;
+                if (seg != kNoKey) tp = atomicMin(a.best + static_cast<uint64_t>(rp) * kLanes + lane, seg) == kNoKey;
+                touch(a, tp, rp, tl);
+            }
+            // bridges: one warp per edge
+            for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) edge_lanes(a, i, allmask, r, flat, mj, tl, wlo);
+        } else {
+            const uint32_t cnt = __ldcg(a.ctr + par);
+            const uint32_t* in = a.wl + static_cast<uint64_t>(par) * a.E;
+            for (uint32_t t = gw; t < cnt; t += nw) {
+                const uint32_t i = __ldcg(in + t);
+                edge_lanes(a, i, __ldcg(a.live + i), r, flat, mj, tl, wlo);
+            }
+        }
+        tl.flush();
+        wlo.flush();
+        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        const uint32_t tcount = __ldcg(a.ctr + 2 + par);
+        if (tcount == 0) break;
+        // ---- phase B
+        for (uint32_t t = gw; t < tcount; t += nw) {
+            const uint32_t c = __ldcg(a.tlist + t);
+            if (lane == 0) a.tflag[c] = 0;
+            unsigned long long* slot = a.best + static_cast<uint64_t>(c) * kLanes + lane;
+            const unsigned long long key = __ldcg(slot);
+            if (key != kNoKey) {
+                *slot = kNoKey;
+                const uint32_t i = static_cast<uint32_t>(key);
+                const uint32_t bit = 1u << lane;
+                if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.ctr[par] = 0;                  // this round's input, consumed
+            a.ctr[2 + ((r + 1) & 1)] = 0;    // next round's touched count
+        }
+        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        // ---- flatten the forests when the next round has enough work to profit
+        const uint32_t next = r == 0 ? a.E : __ldcg(a.ctr + ((r + 1) & 1));
+        flat = a.flatten_div != 0 && static_cast<uint64_t>(next) * a.flatten_div > a.n;
+        if (flat) {
+            for (uint32_t v = gw; v < a.n; v += nw) {
+                if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = find32(a.parent, v, lane);
+            }
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        }
+    }
+    if (r == kMaxRounds) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusRoundLimit);
+        return;
+    }
+    // final flatten: parent[v][j] = root (the component's smallest node)
+    for (uint32_t v = gw; v < a.n; v += nw) {
+        if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = find32(a.parent, v, lane);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[4] = static_cast<uint32_t>(r + 1);
+}
+
+__global__ void k_identity32(uint32_t* __restrict__ parent, uint32_t n) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < static_cast<uint64_t>(n) * kLanes) parent[t] = static_cast<uint32_t>(t / kLanes);
+}
+
+// ---- labels, numbered by each component's smallest node --------------------------------
+// roots after the final flatten: parent[v][j] == v.  One warp per chunk of 32 nodes,
+// lane j counts MST j's roots; the counts are scanned per MST; then lane j numbers its
+// roots and every node takes its root's number (written MST-major through a shared
+// transpose so the stores are coalesced).
+
+__global__ void k_lab_count(const uint32_t* __restrict__ parent, uint32_t n, uint32_t K, uint32_t nchunks,
+                            uint32_t* __restrict__ cc) {
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (chunk >= nchunks) return;
+    uint32_t cnt = 0;
+    for (uint32_t t = 0; t < 32; ++t) {
+        const uint32_t v = chunk * 32 + t;
+        if (v < n && lane < K && parent[static_cast<uint64_t>(v) * kLanes + lane] == v) ++cnt;
+    }
+    if (lane < K) cc[static_cast<uint64_t>(lane) * nchunks + chunk] = cnt;
+}
+
+__global__ void k_lab_roots(const uint32_t* __restrict__ parent, uint32_t n, uint32_t K, uint32_t nchunks,
+                            const uint32_t* __restrict__ cc, uint32_t* __restrict__ rootlab) {
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (chunk >= nchunks || lane >= K) return;
+    uint32_t next = cc[static_cast<uint64_t>(lane) * nchunks + chunk];
+    for (uint32_t t = 0; t < 32; ++t) {
+        const uint32_t v = chunk * 32 + t;
+        if (v < n && parent[static_cast<uint64_t>(v) * kLanes + lane] == v) rootlab[static_cast<uint64_t>(v) * kLanes + lane] = next++;
+    }
+}
+
+__global__ void k_lab_write(const uint32_t* __restrict__ parent, uint32_t n, uint32_t K, uint32_t nchunks,
+                            const uint32_t* __restrict__ rootlab, uint32_t* __restrict__ lab) {
+    __shared__ uint32_t tile[kThreads / 32][32][33];
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    if (chunk >= nchunks) return;
+    for (uint32_t t = 0; t < 32; ++t) {
+        const uint32_t v = chunk * 32 + t;
+        uint32_t x = 0;
+        if (v < n && lane < K) x = rootlab[static_cast<uint64_t>(parent[static_cast<uint64_t>(v) * kLanes + lane]) * kLanes + lane];
+        tile[w][t][lane] = x;  // [node][mst]
+    }
+    __syncwarp();
+    const uint32_t v = chunk * 32 + lane;
+    for (uint32_t j = 0; j < K; ++j) {
+        if (v < n) lab[static_cast<uint64_t>(j) * n + v] = tile[w][lane][j];
+    }
+}
+
+// ---- trees: bit-packed membership -> per-MST edge lists in ascending edge index ----------
+
+__global__ void k_tree_count(const uint32_t* __restrict__ tree, uint32_t E, uint32_t K, uint32_t nchunks,
+                             uint32_t* __restrict__ tc) {
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (chunk >= nchunks) return;
+    uint32_t cnt = 0;
+    for (uint32_t g = 0; g < kChunkEdges / 32; ++g) {
+        const uint32_t i = chunk * kChunkEdges + g * 32 + lane;
+        const uint32_t m = i < E ? tree[i] : 0u;
+        for (uint32_t j = 0; j < K; ++j) {
+            const unsigned b = __ballot_sync(0xFFFFFFFFu, (m >> j) & 1u);
+            if (lane == j) cnt += __popc(b);
+        }
+    }
+    if (lane < K) tc[static_cast<uint64_t>(lane) * nchunks + chunk] = cnt;
+}
+
+__global__ void k_tree_emit(const uint32_t* __restrict__ tree, uint32_t E, uint32_t K, uint32_t nchunks,
+                            const uint32_t* __restrict__ tc, const uint32_t* __restrict__ eu,
+                            const uint32_t* __restrict__ ev, const float* __restrict__ ew,
+                            const float* __restrict__ dists, const uint32_t* __restrict__ counts, uint32_t k,
+                            const uint32_t* __restrict__ mpts, uint64_t cap, cs_edge* __restrict__ out, int* status) {
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (chunk >= nchunks) return;
+    uint32_t off = lane < K ? tc[static_cast<uint64_t>(lane) * nchunks + chunk] : 0u;
+    for (uint32_t g = 0; g < kChunkEdges / 32; ++g) {
+        const uint32_t i = chunk * kChunkEdges + g * 32 + lane;
+        const uint32_t m = i < E ? tree[i] : 0u;
+        uint32_t u = 0, v = 0, cu = 0, cv = 0;
+        float w = 0.0f;
+        if (m) {
+            u = eu[i];
+            v = ev[i];
+            w = ew[i];
+            cu = counts[u];
+            cv = counts[v];
+        }
+        for (uint32_t j = 0; j < K; ++j) {
+            const bool has = (m >> j) & 1u;
+            const unsigned b = __ballot_sync(0xFFFFFFFFu, has);
+            if (!b) continue;
+            const uint32_t base = __shfl_sync(0xFFFFFFFFu, off, j);
+            if (has) {
+                const uint32_t mj = mpts[j];
+                const float inf = __int_as_float(0x7f800000);
+                const float c1 = cu ? dists[static_cast<uint64_t>(u) * k + (mj < cu ? mj : cu) - 1] : inf;
+                const float c2 = cv ? dists[static_cast<uint64_t>(v) * k + (mj < cv ? mj : cv) - 1] : inf;
+                const uint64_t pos = base + __popc(b & ((1u << lane) - 1u));
+                if (pos < cap) {
+                    cs_edge e;
+                    e.u = u;
+                    e.v = v;
+                    e.w = max_ref(w, max_ref(c1, c2));
+                    out[static_cast<uint64_t>(j) * cap + pos] = e;
+                } else {
+                    atomicOr(status, kStatusCapacity);
+                }
+            }
+            if (lane == j) off += __popc(b);
+        }
+    }
+}
+
+/// Exact weight bins of each tree (per-exponent mantissa sums), one MST per block row.
+__global__ void k_tree_weight(const cs_edge* __restrict__ out, uint64_t cap, const unsigned long long* __restrict__ nedges,
+                              unsigned long long* __restrict__ bins) {
+    __shared__ unsigned long long sb[256];
+    const uint32_t j = blockIdx.y;
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) sb[b] = 0;
+    __syncthreads();
+    const uint64_t ne = nedges[j] < cap ? nedges[j] : cap;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < ne; t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t bits = __float_as_uint(out[static_cast<uint64_t>(j) * cap + t].w);
+        const uint32_t e = (bits >> 23) & 0xFFu;
+        atomicAdd(sb + (e ? e : 1u), static_cast<unsigned long long>((bits & 0x7FFFFFu) | (e ? 0x800000u : 0u)));
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+        if (sb[b]) atomicAdd(bins + static_cast<uint64_t>(j) * 256 + b, sb[b]);
+    }
+}
+
+}  // namespace
+
+// ============================================================================
+// plans: buffers + the three captured graphs of one (graph, K<=32, shape)
+// ============================================================================
+
+struct SweepPlan {
+    uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
+    bool labels = false;
+    uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
+    DevBuf mpts, parent, best, tree, live, wl, tlist, tflag, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins;
+    cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
+    std::vector<uint32_t> host_mpts;
+    const void* key_ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
+    float last_graph_ms = 0.0f, last_kernel_ms = 0.0f;
+    uint32_t last_rounds = 0;
+    SweepPlan* next = nullptr;  // the following pass of a sweep with K > 32
+    ~SweepPlan() {
+        if (exec_pre) cudaGraphExecDestroy(exec_pre);
+        if (exec_main) cudaGraphExecDestroy(exec_main);
+        if (exec_post) cudaGraphExecDestroy(exec_post);
+        if (ev_k0) cudaEventDestroy(ev_k0);
+        if (ev_k1) cudaEventDestroy(ev_k1);
+        delete next;
+    }
+};
+
+void sweep_free(SweepPlan* p) { delete p; }
+
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, std::pair<uint32_t, uint32_t>> g_tuned;  // -> (block, flatten_div)
+
+SweepArgs args_of(Graph& g, SweepPlan& p) {
+    SweepArgs a;
+    a.n = p.n;
+    a.E = p.E;
+    a.e_knn = p.e_knn;
+    a.K = p.K;
+    a.k = g.k;
+    a.flatten_div = p.flatten_div;
+    a.eu = g.eu.as<uint32_t>();
+    a.ev = g.ev.as<uint32_t>();
+    a.ew = g.ew.as<float>();
+    a.node_off = g.node_off.as<uint32_t>();
+    a.dists = g.dists.as<float>();
+    a.counts = g.counts.as<uint32_t>();
+    a.mpts = p.mpts.as<uint32_t>();
+    a.parent = p.parent.as<uint32_t>();
+    a.best = p.best.as<unsigned long long>();
+    a.tree = p.tree.as<uint32_t>();
+    a.live = p.live.as<uint32_t>();
+    a.wl = p.wl.as<uint32_t>();
+    a.tlist = p.tlist.as<uint32_t>();
+    a.tflag = p.tflag.as<uint32_t>();
+    a.ctr = p.ctr.as<uint32_t>();
+    a.bar = p.bar.as<unsigned>();
+    a.status = p.status.as<int>();
+    a.limit_ns = kBarrierLimitNs;
+    return a;
+}
+
+/// pre: reset the per-sweep state.
+void enqueue_pre(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    const uint64_t n = std::max<uint32_t>(p.n, 1), E = std::max<uint32_t>(p.E, 1);
+    CSB_CUDA(cudaMemsetAsync(p.status.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.bar.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.ctr.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.best.p, 0xFF, n * kLanes * 8, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.tree.p, 0, E * 4, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.tflag.p, 0, n * 4, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.bins.p, 0, static_cast<uint64_t>(p.K) * 256 * 8, c.stream));
+    k_identity32<<<blocks_for(n * kLanes), kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n);
+    count_launch(c);
+}
+
+void enqueue_main(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    SweepArgs a = args_of(g, p);
+    void* params[] = {&a};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.grid);
+    cfg.blockDim = dim3(p.block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CSB_CUDA(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void*>(k_sweep), params));
+    count_launch(c);
+}
+
+/// post: labels (optional), tree lists, exact weight bins.
+void enqueue_post(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    const unsigned wpb = kThreads / 32;
+    unsigned long long* nedges = p.counts.as<unsigned long long>();
+    unsigned long long* ncomp = nedges + 32;
+    if (p.labels) {
+        const unsigned gb = static_cast<unsigned>((p.ncn + wpb - 1) / wpb);
+        k_lab_count<<<gb, kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n, p.K, p.ncn, p.cc.as<uint32_t>());
+        count_launch(c);
+        launch_scan_tiles(c, p.cc.as<uint32_t>(), p.ncn, p.K, ncomp);
+        k_lab_roots<<<gb, kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n, p.K, p.ncn, p.cc.as<uint32_t>(),
+                                                  p.rootlab.as<uint32_t>());
+        k_lab_write<<<gb, kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n, p.K, p.ncn, p.rootlab.as<uint32_t>(),
+                                                  p.lab.as<uint32_t>());
+        count_launch(c, 2);
+    }
+    const unsigned ge = static_cast<unsigned>((p.nce + wpb - 1) / wpb);
+    k_tree_count<<<ge, kThreads, 0, c.stream>>>(p.tree.as<uint32_t>(), p.E, p.K, p.nce, p.tcnt.as<uint32_t>());
+    count_launch(c);
+    launch_scan_tiles(c, p.tcnt.as<uint32_t>(), p.nce, p.K, nedges);
+    const uint64_t cap = p.n ? p.n - 1 : 0;
+    k_tree_emit<<<ge, kThreads, 0, c.stream>>>(p.tree.as<uint32_t>(), p.E, p.K, p.nce, p.tcnt.as<uint32_t>(),
+                                              g.eu.as<uint32_t>(), g.ev.as<uint32_t>(), g.ew.as<float>(),
+                                              g.dists.as<float>(), g.counts.as<uint32_t>(), g.k, p.mpts.as<uint32_t>(),
+                                              cap, p.out.as<cs_edge>(), p.status.as<int>());
+    dim3 gw(std::max<unsigned>(1, std::min<unsigned>(64, blocks_for(cap))), p.K);
+    k_tree_weight<<<gw, kThreads, 0, c.stream>>>(p.out.as<cs_edge>(), cap, nedges, p.bins.as<unsigned long long>());
+    count_launch(c, 2);
+}
+
+using Enqueue = void (*)(Graph&, SweepPlan&);
+
+bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
+    Ctx& c = *g.ctx;
+    *out = nullptr;
+    if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const uint64_t before = c.launches;
+    bool ok = true;
+    try {
+        f(g, p);
+    } catch (...) {
+        ok = false;
+    }
+    c.launches = before;  // counted when replayed
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+    ok = ok && e == cudaSuccess && graph;
+    if (ok) ok = cudaGraphInstantiate(out, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        cudaGetLastError();
+        *out = nullptr;
+    }
+    return ok;
+}
+
+uint64_t kernels_pre() { return 1; }
+uint64_t kernels_post(const SweepPlan& p) { return (p.labels ? 4 : 0) + 4; }
+
+SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div, bool labels) {
+    Ctx& c = *g.ctx;
+    SweepPlan* p = new SweepPlan();
+    try {
+        p->n = static_cast<uint32_t>(g.n);
+        p->E = static_cast<uint32_t>(g.e_total);
+        p->e_knn = static_cast<uint32_t>(g.e_knn);
+        p->K = K;
+        p->block = block;
+        p->flatten_div = flatten_div;
+        p->labels = labels;
+        p->key_ptrs[0] = g.eu.p;
+        p->key_ptrs[1] = g.ev.p;
+        p->key_ptrs[2] = g.ew.p;
+        p->key_ptrs[3] = g.dists.p;
+        p->key_ptrs[4] = g.counts.p;
+        p->key_ptrs[5] = g.node_off.p;
+        const uint64_t n = std::max<uint32_t>(p->n, 1), E = std::max<uint32_t>(p->E, 1);
+        p->ncn = static_cast<uint32_t>((n + 31) / 32);
+        p->nce = static_cast<uint32_t>((E + kChunkEdges - 1) / kChunkEdges);
+        p->mpts.ensure(32 * 4);
+        p->parent.ensure(n * kLanes * 4);
+        p->best.ensure(n * kLanes * 8);
+        p->tree.ensure(E * 4);
+        p->live.ensure(E * 4);
+        p->wl.ensure(2 * E * 4);
+        p->tlist.ensure(n * 4);
+        p->tflag.ensure(n * 4);
+        p->ctr.ensure(64);
+        p->bar.ensure(64);
+        p->status.ensure(64);
+        p->cc.ensure(static_cast<uint64_t>(K) * p->ncn * 4 + 64);
+        p->tcnt.ensure(static_cast<uint64_t>(K) * p->nce * 4 + 64);
+        if (labels) {
+            p->rootlab.ensure(n * kLanes * 4);
+            p->lab.ensure(static_cast<uint64_t>(K) * n * 4);
+        }
+        p->out.ensure(static_cast<uint64_t>(K) * std::max<uint64_t>(n - 1, 1) * sizeof(cs_edge));
+        p->counts.ensure(64 * 8);
+        p->bins.ensure(static_cast<uint64_t>(K) * 256 * 8);
+        CSB_CUDA(cudaEventCreate(&p->ev_k0));
+        CSB_CUDA(cudaEventCreate(&p->ev_k1));
+        int occ = 0;
+        CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep, static_cast<int>(block), 0));
+        if (occ < 1) fail(CS_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
+        p->grid = static_cast<uint32_t>(c.sm_count) * static_cast<uint32_t>(occ);
+        capture_part(g, *p, enqueue_pre, &p->exec_pre);
+        capture_part(g, *p, enqueue_main, &p->exec_main);
+        capture_part(g, *p, enqueue_post, &p->exec_post);
+    } catch (...) {
+        delete p;
+        throw;
+    }
+    return p;
+}
+
+void status_check(Ctx& c, const int* d_status) {
+    int st = 0;
+    CSB_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    if (st & kStatusBarrierTimeout) fail(CS_ERR_TIMEOUT, "MST sweep: a grid barrier wait ran out");
+    if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "MST sweep: a union retry loop ran out");
+    if (st & kStatusRoundLimit) fail(CS_ERR_TIMEOUT, "MST sweep: Boruvka round limit reached");
+    if (st & kStatusCapacity) fail(CS_ERR_STATE, "MST sweep: tree larger than n-1 edges (inconsistent state)");
+}
+
+/// Run one pass (K <= 32): replay pre / main / post with events around main.
+void run_pass(Graph& g, SweepPlan& p) {
+    Ctx& c = *g.ctx;
+    CSB_CUDA(cudaMemcpyAsync(p.mpts.p, p.host_mpts.data(), p.K * 4, cudaMemcpyHostToDevice, c.stream));
+    if (p.exec_pre) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_pre, c.stream));
+        count_launch(c, kernels_pre());
+    } else {
+        enqueue_pre(g, p);
+    }
+    CSB_CUDA(cudaEventRecord(p.ev_k0, c.stream));
+    if (p.exec_main) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_main, c.stream));
+        count_launch(c, 1);
+    } else {
+        enqueue_main(g, p);
+    }
+    CSB_CUDA(cudaEventRecord(p.ev_k1, c.stream));
+    if (p.exec_post) {
+        CSB_CUDA(cudaGraphLaunch(p.exec_post, c.stream));
+        count_launch(c, kernels_post(p));
+    } else {
+        enqueue_post(g, p);
+    }
+}
+
+bool plan_matches(const SweepPlan* p, const Graph& g, uint32_t K, uint32_t block, uint32_t fdiv, bool labels) {
+    return p && p->n == g.n && p->E == g.e_total && p->e_knn == g.e_knn && p->K == K && p->block == block &&
+           p->flatten_div == fdiv && p->labels == labels && p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
+           p->key_ptrs[2] == g.ew.p && p->key_ptrs[3] == g.dists.p && p->key_ptrs[4] == g.counts.p &&
+           p->key_ptrs[5] == g.node_off.p;
+}
+
+}  // namespace
+
+void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms) {
+    if (K == 0) fail(CS_ERR_INVALID, "sweep: K must be positive");
+    for (uint32_t j = 0; j < K; ++j) {
+        if (mpts[j] > g.k) fail(CS_ERR_INVALID, "sweep: mpts exceeds k_max");
+    }
+    if (g.n == 0) fail(CS_ERR_STATE, "sweep: empty graph");
+    graph_build_edges(g);
+    Ctx& c = *g.ctx;
+    uint32_t B = g.sweep_block, F = g.sweep_flatten;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(std::make_tuple(static_cast<uint32_t>(g.n), static_cast<uint32_t>(g.e_total), K, c.sm_count));
+        if (it != g_tuned.end()) {
+            if (!B) B = it->second.first;
+            if (F == kFlattenAuto) F = it->second.second;
+        }
+    }
+    if (!B) B = 512;
+    if (F == kFlattenAuto) F = 4;
+    // passes of at most 32 MSTs, chained plans
+    SweepPlan** slot = &g.plan;
+    for (uint32_t off = 0; off < K; off += kLanes) {
+        const uint32_t Kp = std::min<uint32_t>(kLanes, K - off);
+        if (!plan_matches(*slot, g, Kp, B, F, want_labels)) {
+            SweepPlan* nxt = *slot ? (*slot)->next : nullptr;
+            if (*slot) (*slot)->next = nullptr;
+            sweep_free(*slot);
+            *slot = make_plan(g, Kp, B, F, want_labels);
+            (*slot)->next = nxt;
+        }
+        (*slot)->host_mpts.assign(mpts + off, mpts + off + Kp);
+        for (auto& m : (*slot)->host_mpts) {
+            if (m == 0) m = 1;  // CoreSG::edges treats mpts 0 as 1
+        }
+        slot = &(*slot)->next;
+    }
+    // drop plans of passes this sweep does not use
+    sweep_free(*slot);
+    *slot = nullptr;
+    g.sweep_K = K;
+    cudaEvent_t e0, e1;
+    CSB_CUDA(cudaEventCreate(&e0));
+    CSB_CUDA(cudaEventCreate(&e1));
+    CSB_CUDA(cudaEventRecord(e0, c.stream));
+    for (SweepPlan* p = g.plan; p; p = p->next) run_pass(g, *p);
+    CSB_CUDA(cudaEventRecord(e1, c.stream));
+    CSB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    float kms = 0.0f;
+    for (SweepPlan* p = g.plan; p; p = p->next) {
+        float x = 0.0f;
+        CSB_CUDA(cudaEventElapsedTime(&x, p->ev_k0, p->ev_k1));
+        kms += x;
+        status_check(c, p->status.as<int>());
+        uint32_t rounds = 0;
+        CSB_CUDA(cudaMemcpy(&rounds, p->ctr.as<uint32_t>() + 4, 4, cudaMemcpyDeviceToHost));
+        p->last_rounds = rounds;
+    }
+    g.plan->last_graph_ms = ms;
+    g.plan->last_kernel_ms = kms;
+    if (out_ms) *out_ms = ms;
+}
+
+void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res) {
+    if (!g.plan) fail(CS_ERR_STATE, "sweep_fetch: no sweep has run");
+    if (index >= g.sweep_K) fail(CS_ERR_INVALID, "sweep_fetch: index out of range");
+    SweepPlan* p = g.plan;
+    uint32_t j = index;
+    while (j >= p->K) {
+        j -= p->K;
+        p = p->next;
+    }
+    if (out_labels && !p->labels) fail(CS_ERR_STATE, "sweep_fetch: the sweep ran without labels");
+    Ctx& c = *g.ctx;
+    unsigned long long ne = 0;
+    uint64_t bins[256];
+    CSB_CUDA(cudaMemcpyAsync(&ne, p->counts.as<unsigned long long>() + j, 8, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaMemcpyAsync(bins, p->bins.as<unsigned long long>() + static_cast<uint64_t>(j) * 256, sizeof(bins),
+                             cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    res->nedges = ne;
+    res->ncomp = static_cast<uint32_t>(p->n - ne);
+    res->weight = exact_sum_from_bins(bins);
+    const uint64_t cap = p->n ? p->n - 1 : 0;
+    if (out_edges && ne) copy_d2h(c, out_edges, p->out.as<cs_edge>() + j * cap, ne * sizeof(cs_edge));
+    if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n, static_cast<uint64_t>(p->n) * 4);
+}
+
+}  // namespace csb
+
+// ============================================================================
+// C API
+// ============================================================================
+
+using namespace csb;
+
+extern "C" {
+
+cs_status cs_extract_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
+                           uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
+                           double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep: null mpts");
+        sweep_run(*g, mpts, K, out_labels != nullptr, nullptr);
+        const uint64_t cap = g->n ? g->n - 1 : 0;
+        for (uint32_t j = 0; j < K; ++j) {
+            MstHost r;
+            sweep_fetch(*g, j, out_edges ? out_edges + j * cap : nullptr,
+                        out_labels ? out_labels + static_cast<uint64_t>(j) * g->n : nullptr, &r);
+            if (out_nedges) out_nedges[j] = r.nedges;
+            if (out_ncomp) out_ncomp[j] = r.ncomp;
+            if (out_weight) out_weight[j] = r.weight;
+        }
+    });
+}
+
+cs_status cs_extract_sweep_device(cs_graph* gp, const uint32_t* mpts, uint32_t K, float* out_ms) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep_device: null mpts");
+        sweep_run(*g, mpts, K, true, out_ms);
+    });
+}
+
+cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
+                         uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        MstHost r;
+        sweep_fetch(*g, index, out_edges, out_labels, &r);
+        if (out_nedges) *out_nedges = r.nedges;
+        if (out_ncomp) *out_ncomp = r.ncomp;
+        if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_sweep_timing(cs_graph* gp, float* graph_ms, float* kernel_ms) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        if (!g->plan) fail(CS_ERR_STATE, "cs_sweep_timing: no sweep has run");
+        if (graph_ms) *graph_ms = g->plan->last_graph_ms;
+        if (kernel_ms) *kernel_ms = g->plan->last_kernel_ms;
+    });
+}
+
+cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t flatten_div, uint32_t block_threads) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(block_threads == 0 || block_threads == 128 || block_threads == 256 || block_threads == 512,
+                    "cs_set_sweep_shape: block must be 128, 256 or 512");
+        g->sweep_block = block_threads;
+        g->sweep_flatten = flatten_div == 0 ? kFlattenAuto : (flatten_div == 0xFFFFFFFFu ? 0 : flatten_div);
+    });
+}
+
+cs_status cs_autotune_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, uint32_t* out_flatten,
+                            uint32_t* out_block) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(mpts != nullptr && K > 0, "cs_autotune_sweep: empty mpts");
+        const uint32_t saved_b = g->sweep_block, saved_f = g->sweep_flatten;
+        float best_ms = 1e30f;
+        uint32_t best_b = 512, best_f = 4;
+        const uint32_t blocks[] = {256, 512};
+        const uint32_t flats[] = {0, 2, 4, 16};
+        for (uint32_t B : blocks) {
+            for (uint32_t F : flats) {
+                g->sweep_block = B;
+                g->sweep_flatten = F;
+                float ms = 0.0f, tot = 0.0f;
+                sweep_run(*g, mpts, K, true, &ms);  // plan + warm
+                for (int rep = 0; rep < 2; ++rep) {
+                    sweep_run(*g, mpts, K, true, &ms);
+                    tot += ms;
+                }
+                if (tot < best_ms) {
+                    best_ms = tot;
+                    best_b = B;
+                    best_f = F;
+                }
+            }
+        }
+        g->sweep_block = saved_b;
+        g->sweep_flatten = saved_f;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tuned[std::make_tuple(static_cast<uint32_t>(g->n), static_cast<uint32_t>(g->e_total), K, g->ctx->sm_count)] =
+                std::make_pair(best_b, best_f);
+        }
+        if (out_flatten) *out_flatten = best_f;
+        if (out_block) *out_block = best_b;
+    });
+}
+
+}  // extern "C"
