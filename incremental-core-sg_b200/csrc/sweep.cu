@@ -100,6 +100,18 @@ __device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_
     }
 }
 
+/// Root of x in forest j without writing: the flatten passes use it, so that every
+/// entry a flatten writes is its own node's, and only ever the final root (path
+/// halving there would race with other nodes' flatten writes and could put back a
+/// stale intermediate ancestor after the root was written).
+__device__ __forceinline__ uint32_t root32(const uint32_t* parent, uint32_t x, uint32_t j) {
+    for (;;) {
+        const uint32_t p = __ldcg(parent + static_cast<uint64_t>(x) * kLanes + j);
+        if (p == x) return x;
+        x = p;
+    }
+}
+
 __device__ __forceinline__ bool unite32(uint32_t* parent, uint32_t a, uint32_t b, uint32_t j, int* status) {
     for (int it = 0; it < (1 << 20); ++it) {
         a = find32(parent, a, j);
@@ -280,7 +292,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         flat = a.flatten_div != 0 && static_cast<uint64_t>(next) * a.flatten_div > a.n;
         if (flat) {
             for (uint32_t v = gw; v < a.n; v += nw) {
-                if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = find32(a.parent, v, lane);
+                if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
             }
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
@@ -291,7 +303,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     }
     // final flatten: parent[v][j] = root (the component's smallest node)
     for (uint32_t v = gw; v < a.n; v += nw) {
-        if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = find32(a.parent, v, lane);
+        if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[4] = static_cast<uint32_t>(r + 1);
 }
@@ -780,10 +792,11 @@ void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_lab
     CSB_CUDA(cudaMemcpyAsync(bins, p->bins.as<unsigned long long>() + static_cast<uint64_t>(j) * 256, sizeof(bins),
                              cudaMemcpyDeviceToHost, c.stream));
     CSB_CUDA(cudaStreamSynchronize(c.stream));
+    const uint64_t cap = p->n ? p->n - 1 : 0;
+    if (ne > cap) fail(CS_ERR_STATE, "sweep_fetch: the last sweep did not complete");
     res->nedges = ne;
     res->ncomp = static_cast<uint32_t>(p->n - ne);
     res->weight = exact_sum_from_bins(bins);
-    const uint64_t cap = p->n ? p->n - 1 : 0;
     if (out_edges && ne) copy_d2h(c, out_edges, p->out.as<cs_edge>() + j * cap, ne * sizeof(cs_edge));
     if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n, static_cast<uint64_t>(p->n) * 4);
 }
