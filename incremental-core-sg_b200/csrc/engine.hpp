@@ -112,6 +112,11 @@ struct Graph {
     DevBuf eu, ev, ew;    // SoA u32/u32/f32 [e_total]
     DevBuf node_off;      // u32 [n+1] offsets of each node's emitted edges
 
+    // Workspace of the plain per-mpts path (mst.cu), kept across calls.
+    struct PlainWork {
+        DevBuf eu, ev, ew, core, parent, best, touched, wl, bitmap, bins, ctr, tiles, lab, out, counts;
+    } plain;
+
     // Hubness selection of the last cs_select_bridges.
     std::vector<uint32_t> selected;
 

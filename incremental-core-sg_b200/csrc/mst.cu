@@ -434,11 +434,13 @@ void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_la
     if (mpts == 0) mpts = 1;
     if (mpts > g.k) fail(CS_ERR_INVALID, "CoreSG::edges: mpts exceeds k_max");
     // edges(mpts), materialised and reweighted (the reference rebuilds them per call)
-    DevBuf eu, ev, ew, core;
+    Graph::PlainWork& pw = g.plain;
+    DevBuf &eu = pw.eu, &ev = pw.ev, &ew = pw.ew, &core = pw.core;
     const uint64_t E = graph_materialize_edges(g, mpts, true, eu, ev, ew, core, c.scratch[0],
                                                c.scratch[1], c.scratch[2]);
     const uint32_t W = static_cast<uint32_t>((E + 31) / 32) + 1;
-    DevBuf parent, best, touched, wl, bitmap, bins, ctr, tiles, lab, outb;
+    DevBuf &parent = pw.parent, &best = pw.best, &touched = pw.touched, &wl = pw.wl, &bitmap = pw.bitmap,
+           &bins = pw.bins, &ctr = pw.ctr, &tiles = pw.tiles, &lab = pw.lab, &outb = pw.out;
     parent.ensure(std::max<uint64_t>(n, 1) * 4);
     best.ensure(std::max<uint64_t>(n, 1) * 8);
     touched.ensure(std::max<uint64_t>(n, 1) * 4);
@@ -495,7 +497,7 @@ void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_la
     }
     if (r == kMaxRounds) fail(CS_ERR_TIMEOUT, "MST: Boruvka round limit reached");
 
-    DevBuf counts;
+    DevBuf& counts = pw.counts;
     counts.ensure(64);
     unsigned long long* d_ncomp = counts.as<unsigned long long>();
     unsigned long long* d_nedges = d_ncomp + 1;
