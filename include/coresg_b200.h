@@ -138,6 +138,13 @@ cs_status cs_graph_get_bridges(cs_graph* g, cs_edge* out, uint64_t cap, uint64_t
 cs_status cs_graph_info(cs_graph* g, uint64_t* n, uint32_t* k_max, uint32_t* dim,
                         uint32_t* stride, uint64_t* knn_edges, uint64_t* bridges);
 
+/* CORESG01 files, byte-compatible with CoreSG::save / CoreSG::load
+ * (src/io.cpp:195-330): padded rows, k-NN arrays, bridges, repair count.
+ * Connectivity and hubness are derived state and are not stored (as in the
+ * reference); cs_select_bridges recomputes them. */
+cs_status cs_graph_save(cs_graph* g, const char* path);
+cs_status cs_graph_load(cs_ctx* ctx, const char* path, cs_graph** out_graph);
+
 /* ---- build: NN-Descent on the resident points + bridges --------------------- */
 
 /* k-NN graph of the resident points by Dynamic NN-Descent (IncrementalKnn::build

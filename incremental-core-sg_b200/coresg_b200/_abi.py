@@ -58,6 +58,8 @@ _SIGS = {
     "cs_graph_set_bridges": (_i32, [_p, _p, _u64]),
     "cs_graph_get_bridges": (_i32, [_p, _p, _u64, _p]),
     "cs_graph_info": (_i32, [_p, _p, _p, _p, _p, _p, _p]),
+    "cs_graph_save": (_i32, [_p, C.c_char_p]),
+    "cs_graph_load": (_i32, [_p, C.c_char_p, _pp]),
     "cs_knn_build": (_i32, [_p, _u32, _u32, _f64, _u64, _p, _p]),
     "cs_select_bridges": (_i32, [_p, _p, _p, _p, _p]),
     "cs_get_selected": (_i32, [_p, _p, _u64, _p]),
@@ -242,6 +244,21 @@ class CoreSG:
         self.ctx.check(lib().cs_graph_info(self.h, C.byref(n), C.byref(k), C.byref(d), C.byref(s),
                                            C.byref(nk), C.byref(nb)))
         return dict(n=n.value, k_max=k.value, dim=d.value, stride=s.value, knn_edges=nk.value, bridges=nb.value)
+
+    def save(self, path: str):
+        """CoreSG::save (CORESG01, src/io.cpp:232-261)."""
+        self.ctx.check(lib().cs_graph_save(self.h, path.encode()))
+
+    @classmethod
+    def load(cls, ctx: Context, path: str) -> "CoreSG":
+        """CoreSG::load (CORESG01, src/io.cpp:263-330)."""
+        h = C.c_void_p()
+        ctx.check(lib().cs_graph_load(ctx.h, path.encode(), C.byref(h)))
+        obj = cls.__new__(cls)
+        obj.ctx, obj.h = ctx, h
+        info = obj.info()
+        obj.dim, obj.k_max = info["dim"], info["k_max"]
+        return obj
 
     @property
     def n(self) -> int:
