@@ -154,6 +154,34 @@ cs_status cs_graph_load(cs_ctx* ctx, const char* path, cs_graph** out_graph);
 cs_status cs_knn_build(cs_graph* g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
                        uint64_t* out_updates, uint32_t* out_rounds);
 
+/* Parameters of cs_insert; cs_insert_defaults fills the reference's defaults
+ * (coresg_cli: sample 16, refine-iters 5, refine-per-new 2.0; IncrementalKnnParams:
+ * refine_max_fraction 0.25, search_ef 2k with 4*ef expansions). */
+typedef struct {
+    uint32_t sample;            /* smpN of the refinement descent */
+    uint32_t refine_iters;      /* rounds of the restricted descent */
+    double refine_per_new;      /* active-set cap per new point (0: no per-point cap) */
+    double refine_max_fraction; /* active-set cap as a fraction of n (>= 1: none) */
+    double delta;               /* stop when a round's updates <= delta * k * |active| */
+    uint32_t max_expand;        /* seeding search expansions per point (0: 8k) */
+    uint64_t seed;
+    int32_t reselect_bridges;   /* 1: re-select the anti-hub bridges afterwards */
+} cs_insert_params;
+void cs_insert_defaults(cs_insert_params* p);
+
+/* Incremental insertion of `count` rows (CoreSG::insert, src/coresg.cpp:325-389 ->
+ * IncrementalKnn::insert, src/incremental_knn.cpp:1155-1252), all on device and over
+ * the one resident graph: the rows are appended; each new point is seeded by a beam
+ * search over the base graph (the anchored seeding search, :118-216); the seeds are
+ * inserted both ways (:1195-1200); a restricted Dynamic NN-Descent runs over the new
+ * points and two rings of their neighbourhoods in discovery order, capped as
+ * refinement_set (:927-987); then, optionally, the bridges are re-selected.  The
+ * reference splits an insert into instances to bound per-device memory; here the
+ * whole graph is resident, so one active set plays every instance.
+ * out_active, out_updates may be NULL. */
+cs_status cs_insert(cs_graph* g, const float* rows, uint64_t count, uint32_t row_stride,
+                    const cs_insert_params* params, uint64_t* out_active, uint64_t* out_updates);
+
 /* Anti-hub bridges for the current k-NN graph, all on device: connectivity
  * (src/connectivity.cpp:99-139), reverse degrees and scores (src/hubness.cpp:44-158,
  * :302-352), selection with the per-component quota (:424-521), the MRD MST over the

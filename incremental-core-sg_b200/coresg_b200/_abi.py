@@ -62,6 +62,8 @@ _SIGS = {
     "cs_graph_load": (_i32, [_p, C.c_char_p, _pp]),
     "cs_knn_build": (_i32, [_p, _u32, _u32, _f64, _u64, _p, _p]),
     "cs_select_bridges": (_i32, [_p, _p, _p, _p, _p]),
+    "cs_insert_defaults": (None, [_p]),
+    "cs_insert": (_i32, [_p, _p, _u64, _u32, _p, _p, _p]),
     "cs_get_selected": (_i32, [_p, _p, _u64, _p]),
     "cs_core_distances": (_i32, [_p, _u32, _p]),
     "cs_edges": (_i32, [_p, _u32, _p, _u64, _p]),
@@ -164,6 +166,12 @@ class Context:
         self.check(lib().cs_mrd_block(self.h, _ptr(pts), m, dim or stride, stride, CS_METRIC_L2,
                                       _ptr(np.ascontiguousarray(core, np.float32)), r0, r1, _ptr(out)))
         return out
+
+
+class InsertParams(C.Structure):
+    _fields_ = [("sample", C.c_uint32), ("refine_iters", C.c_uint32), ("refine_per_new", C.c_double),
+                ("refine_max_fraction", C.c_double), ("delta", C.c_double), ("max_expand", C.c_uint32),
+                ("seed", C.c_uint64), ("reselect_bridges", C.c_int32)]
 
 
 class MstResult:
@@ -283,6 +291,18 @@ class CoreSG:
         out = np.empty(cnt.value, np.uint32)
         self.ctx.check(lib().cs_get_selected(self.h, _ptr(out), cnt.value, C.byref(cnt)))
         return out
+
+    def insert(self, rows: np.ndarray, **params):
+        """CoreSG::insert on the device (cs_insert); params override cs_insert_defaults."""
+        rows = np.ascontiguousarray(rows, np.float32)
+        p = InsertParams()
+        lib().cs_insert_defaults(C.byref(p))
+        for key, val in params.items():
+            setattr(p, key, val)
+        act, upd = C.c_uint64(), C.c_uint64()
+        self.ctx.check(lib().cs_insert(self.h, _ptr(rows), rows.shape[0], rows.shape[1], C.byref(p), C.byref(act),
+                                       C.byref(upd)))
+        return dict(active=act.value, updates=upd.value)
 
     def build(self, rows: np.ndarray, sample=16, iters=10, delta=0.001, seed=42):
         """CoreSG::build: points, NN-Descent, bridges (src/coresg.cpp:260-323)."""

@@ -137,6 +137,9 @@ constexpr uint32_t kFlattenAuto = 0xFFFFFFFEu;
 
 // graph.cu
 void graph_build_edges(Graph& g);  // cached base edge list (no-op when valid)
+/// Upload (or append) n rows of `row_stride` floats as padded points; new nodes
+/// start with empty k-NN lists (Dataset::append + KnnGraph::grow).
+void graph_set_points(Graph& g, const float* rows, uint64_t n, uint32_t row_stride, bool append);
 uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf& u, DevBuf& v,
                                  DevBuf& w, DevBuf& core_out, DevBuf& tmp_mask, DevBuf& tmp_cnt,
                                  DevBuf& tmp_off);
@@ -163,6 +166,13 @@ void launch_scan_tiles(Ctx& c, uint32_t* tiles, uint32_t nt, uint32_t K, unsigne
 // knn.cu
 void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
                  bool random_fill, uint64_t* out_updates, uint32_t* out_rounds);
+struct InsertStats {
+    uint64_t active = 0, updates = 0;
+    uint32_t rounds = 0;
+    double search_ms = 0.0, refine_ms = 0.0;
+};
+void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride, const cs_insert_params& p,
+                InsertStats* st);
 
 // bridges.cu
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,

@@ -289,8 +289,12 @@ void cs_graph_destroy(cs_graph* gp) {
     if (free_ctx) ctx_free(c);
 }
 
-static cs_status set_points_impl(Graph* g, const float* rows, uint64_t n, uint32_t row_stride, bool append) {
-    return guarded(g ? g->ctx : nullptr, [&] {
+}  // extern "C"
+
+namespace csb {
+void graph_set_points(Graph& gr, const float* rows, uint64_t n, uint32_t row_stride, bool append) {
+    Graph* g = &gr;
+    {
         CSB_REQUIRE(rows != nullptr || n == 0, "points: null rows");
         if (row_stride == 0) row_stride = g->dim;
         CSB_REQUIRE(row_stride >= g->dim, "points: row_stride < dim");
@@ -339,7 +343,14 @@ static cs_status set_points_impl(Graph* g, const float* rows, uint64_t n, uint32
             g->n_repair = 0;
         }
         g->invalidate_edges();
-    });
+    }
+}
+}  // namespace csb
+
+extern "C" {
+
+static cs_status set_points_impl(Graph* g, const float* rows, uint64_t n, uint32_t row_stride, bool append) {
+    return guarded(g ? g->ctx : nullptr, [&] { graph_set_points(*g, rows, n, row_stride, append); });
 }
 
 cs_status cs_graph_set_points(cs_graph* gp, const float* rows, uint64_t n, uint32_t row_stride) {

@@ -196,9 +196,11 @@ __global__ void k_sample(uint32_t n, uint32_t k, uint32_t smp, const uint32_t* _
                          uint32_t* __restrict__ new_s, uint32_t* __restrict__ old_s,
                          uint32_t* __restrict__ ns, uint32_t* __restrict__ nold,
                          uint32_t* __restrict__ rnew, uint32_t* __restrict__ rold,
-                         uint32_t* __restrict__ rnew_cnt, uint32_t* __restrict__ rold_cnt) {
-    const uint32_t p = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    if (p >= n) return;
+                         uint32_t* __restrict__ rnew_cnt, uint32_t* __restrict__ rold_cnt,
+                         const uint32_t* __restrict__ active, uint32_t n_active) {
+    const uint32_t w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (w >= (active ? n_active : n)) return;
+    const uint32_t p = active ? active[w] : w;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t c = counts[p];
     const uint32_t max_new = smp, max_old = 3 * smp;
@@ -247,12 +249,14 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
                                                    const uint32_t* __restrict__ rnew_cnt,
                                                    const uint32_t* __restrict__ rold_cnt, const float* __restrict__ thr,
                                                    CandStore cand, int warps_per_block,
-                                                   unsigned long long* __restrict__ evals) {
+                                                   unsigned long long* __restrict__ evals,
+                                                   const uint32_t* __restrict__ active, uint32_t n_active) {
     extern __shared__ float smem[];
     const int w = threadIdx.x >> 5;
     if (w >= warps_per_block) return;
-    const uint32_t p = blockIdx.x * warps_per_block + w;
-    if (p >= n) return;
+    const uint32_t slot = blockIdx.x * warps_per_block + w;
+    if (slot >= (active ? n_active : n)) return;
+    const uint32_t p = active ? active[slot] : slot;
     const unsigned lane = threadIdx.x & 31u;
     constexpr int kRows = kMaxNewList + kMaxOldList;
     // per-warp shared layout: ids[kRows] | thr[kRows] | rows[kRows][stride]
@@ -319,6 +323,13 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
     const uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (u >= n) return;
     const unsigned lane = threadIdx.x & 31u;
+    if (cand.cnt[u] == 0) {  // nothing offered: the list stands; clear the reverse counts
+        if (lane == 0) {
+            rnew_cnt[u] = 0;
+            rold_cnt[u] = 0;
+        }
+        return;
+    }
     unsigned long long key[I];
     uint32_t pay[I];  // bit 0: new flag, bit 1: came from an offer
     const uint32_t c = counts[u];
@@ -430,6 +441,152 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
     }
 }
 
+/// Seeds of new points by beam search over the base graph (IncrementalKnn::search_seeds,
+/// src/incremental_knn.cpp:118-216, forward edges only): one warp per query, a pool of
+/// 64 (rank, id) keys started from 32 random base entries, best-first expansion of the
+/// closest unexpanded pool entry (its k-NN list is scored and merged into the pool by a
+/// 128-element warp bitonic sort), at most max_expand expansions.  Reads the base
+/// graph only; writes the best k pool keys of query t to seeds[t][*].
+__global__ void k_search(const float* __restrict__ pts, uint32_t stride, const uint32_t* __restrict__ ids,
+                         const uint32_t* __restrict__ counts, uint32_t k, uint32_t n_base, uint32_t first_new,
+                         uint32_t count, uint64_t seed, uint32_t max_expand,
+                         unsigned long long* __restrict__ seeds) {
+    extern __shared__ float sq[];
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u, wi = threadIdx.x >> 5;
+    if (t >= count || n_base == 0) return;
+    float* qrow = sq + static_cast<size_t>(wi) * stride;
+    const uint32_t q = first_new + t;
+    for (uint32_t d = lane; d < stride; d += 32) qrow[d] = pts[static_cast<uint64_t>(q) * stride + d];
+    __syncwarp();
+    unsigned long long key[4];
+    uint32_t pay[4];  // bit 0: expanded
+    {
+        const uint64_t h = mix64(seed ^ (0x9E3779B97F4A7C15ull * (q + 1ull)) ^ (0xD6E8FEB86659FD93ull * (lane + 1ull)));
+        const uint32_t e = static_cast<uint32_t>((h >> 32) % n_base);
+        const float r = l2sqr_ref(qrow, pts + static_cast<uint64_t>(e) * stride, stride);
+        unsigned long long ck = make_key(r, e);
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, ck);
+        if (static_cast<int>(lane) != __ffs(same) - 1) ck = kNoKey;
+        key[0] = key[1] = key[3] = kNoKey;
+        key[2] = ck;
+        pay[0] = pay[1] = pay[2] = pay[3] = 0;
+        warp_bitonic<4>(key, pay);
+        key[2] = key[3] = kNoKey;
+    }
+    for (uint32_t it = 0; it < max_expand; ++it) {
+        unsigned long long best = kNoKey;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (key[i] != kNoKey && !(pay[i] & 1u) && key[i] < best) best = key[i];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+            best = x < best ? x : best;
+        }
+        if (best == kNoKey) break;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (key[i] == best) pay[i] |= 1u;
+        }
+        const uint32_t c = static_cast<uint32_t>(best);
+        const uint32_t cnt = counts[c];
+        for (uint32_t b = 0; b < cnt; b += 32) {
+            const uint32_t j = b + lane;
+            const uint32_t nb = j < cnt ? ids[static_cast<uint64_t>(c) * k + j] : kInvalid;
+            bool ok = nb < n_base;
+            unsigned long long ck = kNoKey;
+            if (ok) ck = make_key(l2sqr_ref(qrow, pts + static_cast<uint64_t>(nb) * stride, stride), nb);
+            for (int s2 = 0; s2 < 32; ++s2) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const unsigned long long pk = __shfl_sync(0xFFFFFFFFu, key[i], s2);
+                    if (pk != kNoKey && static_cast<uint32_t>(pk) == nb) ok = false;
+                }
+            }
+            key[2] = ok ? ck : kNoKey;
+            pay[2] = 0;
+            key[3] = kNoKey;
+            pay[3] = 0;
+            if (!__any_sync(0xFFFFFFFFu, ok)) continue;
+            warp_bitonic<4>(key, pay);
+            key[2] = key[3] = kNoKey;
+        }
+    }
+    for (uint32_t e = lane; e < k; e += 32) {
+        const int i = static_cast<int>(e / 32);
+        // element e = i*32 + lane of the sorted pool
+        unsigned long long x = kNoKey;
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii) {
+            if (ii == i) x = key[ii];
+        }
+        seeds[static_cast<uint64_t>(t) * k + e] = x;
+    }
+}
+
+/// Apply the seeds symmetrically: q <- s and s <- q (src/incremental_knn.cpp:1195-1200).
+__global__ void k_apply_seeds(const unsigned long long* __restrict__ seeds, uint32_t count, uint32_t k,
+                              uint32_t first_new, CandStore cand) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= static_cast<uint64_t>(count) * k) return;
+    const unsigned long long key = seeds[x];
+    if (key == kNoKey) return;
+    const uint32_t q = first_new + static_cast<uint32_t>(x / k);
+    const uint32_t s = static_cast<uint32_t>(key);
+    const float r = __uint_as_float(static_cast<uint32_t>(key >> 32));
+    offer(cand, q, make_key(r, s));
+    offer(cand, s, make_key(r, q));
+}
+
+/// One ring of refinement_set (src/incremental_knn.cpp:927-987) in discovery order:
+/// the sequence is (src[t], j) for the list entries of the source nodes in order;
+/// a node joins the ring at its first position in the sequence if unmarked.
+__global__ void k_ring_first(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids,
+                             const uint32_t* __restrict__ counts, uint32_t k, uint32_t n,
+                             const uint8_t* __restrict__ mark, uint32_t* __restrict__ firstpos) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= static_cast<uint64_t>(ns) * k) return;
+    const uint32_t v = src[x / k], j = static_cast<uint32_t>(x % k);
+    if (j >= counts[v]) return;
+    const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
+    if (q < n && !mark[q]) atomicMin(firstpos + q, static_cast<uint32_t>(x));
+}
+
+__global__ void k_ring_flag(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids,
+                            const uint32_t* __restrict__ counts, uint32_t k, uint32_t n,
+                            const uint8_t* __restrict__ mark, const uint32_t* __restrict__ firstpos,
+                            uint32_t* __restrict__ flag) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= static_cast<uint64_t>(ns) * k) return;
+    const uint32_t v = src[x / k], j = static_cast<uint32_t>(x % k);
+    uint32_t f = 0;
+    if (j < counts[v]) {
+        const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
+        f = (q < n && !mark[q] && firstpos[q] == static_cast<uint32_t>(x)) ? 1u : 0u;
+    }
+    flag[x] = f;
+}
+
+__global__ void k_ring_emit(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids, uint32_t k,
+                            const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off, uint32_t limit,
+                            uint8_t* __restrict__ mark, uint32_t* __restrict__ out) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= static_cast<uint64_t>(ns) * k || !flag[x]) return;
+    const uint32_t pos = off[x];
+    if (pos >= limit) return;
+    const uint32_t q = ids[static_cast<uint64_t>(src[x / k]) * k + x % k];
+    mark[q] = 1;
+    out[pos] = q;
+}
+
+__global__ void k_iota_from(uint32_t* __restrict__ out, uint32_t first, uint32_t count, uint8_t* __restrict__ mark) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    out[t] = first + t;
+    mark[first + t] = 1;
+}
+
 struct KnnScratch {
     DevBuf thr, cand, cand_buf, cand_cnt, new_s, old_s, ns, nold, rnew, rold, rnew_cnt, rold_cnt, counters;
 };
@@ -461,94 +618,220 @@ void launch_merge(Ctx& c, Graph& g, KnnScratch& s, unsigned long long* updates) 
 
 }  // namespace
 
+/// One Dynamic NN-Descent session over a resident graph: scratch, rank-space
+/// distances and thresholds on construction; rounds over all nodes or an active list;
+/// metric units again on finish().
+struct Descent {
+    Graph& g;
+    Ctx& c;
+    KnnScratch s;
+    uint32_t n, k, smp;
+    int wpb = 1;
+    size_t smem = 0;
+    unsigned long long* d_updates = nullptr;
+    unsigned long long* d_evals = nullptr;
+
+    Descent(Graph& graph, uint32_t sample) : g(graph), c(*graph.ctx) {
+        n = static_cast<uint32_t>(g.n);
+        k = g.k;
+        smp = std::min<uint32_t>(std::max<uint32_t>(sample, 1), kMaxSample);
+        if (k > 64) fail(CS_ERR_UNSUPPORTED, "NN-Descent: k > 64");
+        const uint64_t nk = static_cast<uint64_t>(n) * k;
+        s.thr.ensure(n * 4ull);
+        s.cand.ensure(n * 8ull * kSlots);
+        s.cand_buf.ensure(n * 8ull * kCap);
+        s.cand_cnt.ensure(n * 4ull);
+        s.new_s.ensure(n * 4ull * kMaxSample);
+        s.old_s.ensure(n * 4ull * 3 * kMaxSample);
+        s.ns.ensure(n * 4ull);
+        s.nold.ensure(n * 4ull);
+        s.rnew.ensure(n * 4ull * kMaxSample);
+        s.rold.ensure(n * 4ull * kMaxSample);
+        s.rnew_cnt.ensure(n * 4ull);
+        s.rold_cnt.ensure(n * 4ull);
+        s.counters.ensure(64);
+        d_updates = s.counters.as<unsigned long long>();
+        d_evals = d_updates + 1;
+        CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
+        CSB_CUDA(cudaMemsetAsync(s.cand_cnt.p, 0, n * 4ull, c.stream));
+        CSB_CUDA(cudaMemsetAsync(s.rnew_cnt.p, 0, n * 4ull, c.stream));
+        CSB_CUDA(cudaMemsetAsync(s.rold_cnt.p, 0, n * 4ull, c.stream));
+        CSB_CUDA(cudaMemsetAsync(s.counters.p, 0, 64, c.stream));
+        k_to_rank<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.dists.as<float>(), nk, g.metric);
+        k_threshold<<<blocks_for(n), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(), n, k,
+                                                             s.thr.as<float>());
+        count_launch(c, 2);
+        // join launch shape: as many warps per block as the staged rows allow
+        constexpr int kRows = kMaxNewList + kMaxOldList;
+        const size_t per_warp = (2 * kRows + static_cast<size_t>(kRows) * g.stride) * 4;
+        wpb = static_cast<int>(std::min<size_t>(kWarps, std::max<size_t>(1, (200u * 1024u) / per_warp)));
+        smem = per_warp * wpb;
+        CSB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        check_launch(c, "NN-Descent setup");
+    }
+
+    /// init_random: top every short list up with random candidates.
+    void random_fill(uint64_t seed) {
+        const unsigned gw = static_cast<unsigned>((n + kWarps - 1) / kWarps);
+        const uint32_t max_attempts = k + k / 2 + 4;
+        for (int pass = 0; pass * 32u < max_attempts; ++pass) {
+            k_random_push<<<gw, kThreads, 0, c.stream>>>(g.pts.as<float>(), n, g.stride, g.counts.as<uint32_t>(), k, seed,
+                                                          pass, store_of(s));
+            count_launch(c);
+            launch_merge(c, g, s, nullptr);
+        }
+        check_launch(c, "NN-Descent random fill");
+    }
+
+    /// Rounds over `active` (all nodes when null) with the delta stop rule.
+    uint64_t rounds(const uint32_t* active, uint32_t n_active, uint32_t iters, double delta, uint32_t* out_rounds) {
+        const uint32_t m = active ? n_active : n;
+        const unsigned gw = static_cast<unsigned>(std::max<uint32_t>(1, (m + kWarps - 1) / kWarps));
+        const unsigned gj = static_cast<unsigned>(std::max<uint32_t>(1, (m + wpb - 1) / wpb));
+        const double stop = delta * static_cast<double>(k) * static_cast<double>(m);
+        uint64_t total = 0;
+        uint32_t done = 0;
+        for (uint32_t it = 0; it < iters && m > 0; ++it) {
+            CSB_CUDA(cudaMemsetAsync(d_updates, 0, 8, c.stream));
+            k_sample<<<gw, kThreads, 0, c.stream>>>(n, k, smp, g.ids.as<uint32_t>(), g.flags.as<uint8_t>(),
+                                                     g.counts.as<uint32_t>(), s.new_s.as<uint32_t>(),
+                                                     s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
+                                                     s.rnew.as<uint32_t>(), s.rold.as<uint32_t>(),
+                                                     s.rnew_cnt.as<uint32_t>(), s.rold_cnt.as<uint32_t>(), active, m);
+            k_join<<<gj, wpb * 32, smem, c.stream>>>(g.pts.as<float>(), n, g.stride, smp, s.new_s.as<uint32_t>(),
+                                                      s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
+                                                      s.rnew.as<uint32_t>(), s.rold.as<uint32_t>(),
+                                                      s.rnew_cnt.as<uint32_t>(), s.rold_cnt.as<uint32_t>(),
+                                                      s.thr.as<float>(), store_of(s), wpb, d_evals, active, m);
+            count_launch(c, 2);
+            launch_merge(c, g, s, d_updates);
+            check_launch(c, "NN-Descent round");
+            unsigned long long upd = 0;
+            CSB_CUDA(cudaMemcpyAsync(&upd, d_updates, 8, cudaMemcpyDeviceToHost, c.stream));
+            CSB_CUDA(cudaStreamSynchronize(c.stream));
+            total += upd;
+            done = it + 1;
+            if (static_cast<double>(upd) <= stop) break;
+        }
+        if (out_rounds) *out_rounds = done;
+        return total;
+    }
+
+    void finish() {
+        const uint64_t nk = static_cast<uint64_t>(n) * k;
+        k_finalize<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.dists.as<float>(), nk, g.metric);
+        count_launch(c);
+        check_launch(c, "NN-Descent finalize");
+        c.sync();
+        g.invalidate_edges();
+    }
+};
+
 /// Dynamic NN-Descent over the graph's resident points and k-NN arrays (which are
 /// the warm start; distances in metric units on entry and exit).
 void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed, bool random_fill,
                  uint64_t* out_updates, uint32_t* out_rounds) {
-    Ctx& c = *g.ctx;
-    const uint32_t n = static_cast<uint32_t>(g.n);
-    if (g.k > 64) fail(CS_ERR_UNSUPPORTED, "NN-Descent: k > 64");
     if (out_updates) *out_updates = 0;
     if (out_rounds) *out_rounds = 0;
-    if (n == 0) return;
-    const uint32_t smp = std::min<uint32_t>(std::max<uint32_t>(sample, 1), kMaxSample);
-    const uint32_t k = g.k;
-    const uint64_t nk = static_cast<uint64_t>(n) * k;
-    KnnScratch s;
-    s.thr.ensure(n * 4ull);
-    s.cand.ensure(n * 8ull * kSlots);
-    s.cand_buf.ensure(n * 8ull * kCap);
-    s.cand_cnt.ensure(n * 4ull);
-    s.new_s.ensure(n * 4ull * kMaxSample);
-    s.old_s.ensure(n * 4ull * 3 * kMaxSample);
-    s.ns.ensure(n * 4ull);
-    s.nold.ensure(n * 4ull);
-    s.rnew.ensure(n * 4ull * kMaxSample);
-    s.rold.ensure(n * 4ull * kMaxSample);
-    s.rnew_cnt.ensure(n * 4ull);
-    s.rold_cnt.ensure(n * 4ull);
-    s.counters.ensure(64);
-    unsigned long long* d_updates = s.counters.as<unsigned long long>();
-    unsigned long long* d_evals = d_updates + 1;
-    CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
-    CSB_CUDA(cudaMemsetAsync(s.cand_cnt.p, 0, n * 4ull, c.stream));
-    CSB_CUDA(cudaMemsetAsync(s.rnew_cnt.p, 0, n * 4ull, c.stream));
-    CSB_CUDA(cudaMemsetAsync(s.rold_cnt.p, 0, n * 4ull, c.stream));
-    CSB_CUDA(cudaMemsetAsync(s.counters.p, 0, 64, c.stream));
-    k_to_rank<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.dists.as<float>(), nk, g.metric);
-    k_threshold<<<blocks_for(n), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(), n, k,
-                                                         s.thr.as<float>());
+    if (g.n == 0) return;
+    Descent d(g, sample);
+    if (random_fill) d.random_fill(seed);
+    const uint64_t upd = d.rounds(nullptr, 0, iters, delta, out_rounds);
+    d.finish();
+    if (out_updates) *out_updates = upd;
+}
+
+/// One ring of refinement_set appended to `out` at `at` (at most `limit` nodes);
+/// returns the ring's size.
+uint32_t expand_ring(Ctx& c, Graph& g, const uint32_t* src, uint32_t ns, uint8_t* mark, uint32_t* firstpos,
+                     DevBuf& flag, DevBuf& off, uint32_t* out, uint32_t limit) {
+    if (ns == 0 || limit == 0) return 0;
+    const uint32_t n = static_cast<uint32_t>(g.n), k = g.k;
+    const uint64_t seq = static_cast<uint64_t>(ns) * k;
+    if (seq > 0xFFFFFFFEull) fail(CS_ERR_UNSUPPORTED, "insert: refinement ring too large");
+    flag.ensure(seq * 4 + 4);
+    off.ensure(seq * 4 + 8);
+    CSB_CUDA(cudaMemsetAsync(firstpos, 0xFF, n * 4ull, c.stream));
+    k_ring_first<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, n,
+                                                            mark, firstpos);
+    k_ring_flag<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, n,
+                                                           mark, firstpos, flag.as<uint32_t>());
     count_launch(c, 2);
-    const unsigned gw = static_cast<unsigned>((n + kWarps - 1) / kWarps);
-    if (random_fill) {
-        const uint32_t max_attempts = k + k / 2 + 4;
-        for (int pass = 0; pass * 32u < max_attempts; ++pass) {
-            k_random_push<<<gw, kThreads, 0, c.stream>>>(g.pts.as<float>(), n, g.stride, g.counts.as<uint32_t>(), k,
-                                                          seed, pass, store_of(s));
-            count_launch(c);
-            launch_merge(c, g, s, nullptr);
-        }
-    }
-    check_launch(c, "NN-Descent init");
-    // join launch shape: as many warps per block as the staged rows allow
-    constexpr int kRows = kMaxNewList + kMaxOldList;
-    const size_t per_warp = (2 * kRows + static_cast<size_t>(kRows) * g.stride) * 4;
-    int wpb = static_cast<int>(std::min<size_t>(kWarps, std::max<size_t>(1, (200u * 1024u) / per_warp)));
-    const size_t smem = per_warp * wpb;
-    CSB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    const unsigned gj = static_cast<unsigned>((n + wpb - 1) / wpb);
-    const double stop = delta * static_cast<double>(k) * static_cast<double>(n);
-    uint64_t total = 0;
-    uint32_t rounds = 0;
-    for (uint32_t it = 0; it < iters; ++it) {
-        CSB_CUDA(cudaMemsetAsync(d_updates, 0, 8, c.stream));
-        k_sample<<<gw, kThreads, 0, c.stream>>>(n, k, smp, g.ids.as<uint32_t>(), g.flags.as<uint8_t>(),
-                                                 g.counts.as<uint32_t>(), s.new_s.as<uint32_t>(), s.old_s.as<uint32_t>(),
-                                                 s.ns.as<uint32_t>(), s.nold.as<uint32_t>(), s.rnew.as<uint32_t>(),
-                                                 s.rold.as<uint32_t>(), s.rnew_cnt.as<uint32_t>(),
-                                                 s.rold_cnt.as<uint32_t>());
-        k_join<<<gj, wpb * 32, smem, c.stream>>>(g.pts.as<float>(), n, g.stride, smp, s.new_s.as<uint32_t>(),
-                                                  s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
-                                                  s.rnew.as<uint32_t>(), s.rold.as<uint32_t>(),
-                                                  s.rnew_cnt.as<uint32_t>(), s.rold_cnt.as<uint32_t>(),
-                                                  s.thr.as<float>(), store_of(s), wpb, d_evals);
-        count_launch(c, 2);
-        launch_merge(c, g, s, d_updates);
-        check_launch(c, "NN-Descent round");
-        unsigned long long upd = 0;
-        CSB_CUDA(cudaMemcpyAsync(&upd, d_updates, 8, cudaMemcpyDeviceToHost, c.stream));
-        CSB_CUDA(cudaStreamSynchronize(c.stream));
-        total += upd;
-        rounds = it + 1;
-        if (static_cast<double>(upd) <= stop) break;
-    }
-    k_finalize<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.dists.as<float>(), nk, g.metric);
+    scan_u32(c, flag.as<uint32_t>(), off.as<uint32_t>(), seq);
+    uint32_t total = 0;
+    CSB_CUDA(cudaMemcpyAsync(&total, off.as<uint32_t>() + seq, 4, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    k_ring_emit<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), k, flag.as<uint32_t>(),
+                                                           off.as<uint32_t>(), limit, mark, out);
     count_launch(c);
-    check_launch(c, "NN-Descent finalize");
-    c.sync();
-    g.invalidate_edges();
-    if (out_updates) *out_updates = total;
-    if (out_rounds) *out_rounds = rounds;
+    check_launch(c, "refinement ring");
+    return std::min(total, limit);
+}
+
+void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride, const cs_insert_params& p,
+                InsertStats* st) {
+    Ctx& c = *g.ctx;
+    if (count == 0) return;
+    CSB_REQUIRE(g.n > 0, "cs_insert: insert before build (CoreSG::insert requires a built graph)");
+    const uint32_t first_new = static_cast<uint32_t>(g.n);
+    graph_set_points(g, rows, count, row_stride, true);
+    const uint32_t n = static_cast<uint32_t>(g.n), k = g.k, nn = static_cast<uint32_t>(count);
+    cudaEvent_t e0, e1, e2;
+    CSB_CUDA(cudaEventCreate(&e0));
+    CSB_CUDA(cudaEventCreate(&e1));
+    CSB_CUDA(cudaEventCreate(&e2));
+    Descent d(g, p.sample);
+    CSB_CUDA(cudaEventRecord(e0, c.stream));
+    // seeding search over the base graph, then the seeds both ways
+    DevBuf seeds;
+    seeds.ensure(static_cast<uint64_t>(nn) * k * 8);
+    const uint32_t max_expand = p.max_expand ? p.max_expand : 8 * k;
+    const size_t qsmem = static_cast<size_t>(kWarps) * g.stride * 4;
+    k_search<<<(nn + kWarps - 1) / kWarps, kThreads, qsmem, c.stream>>>(
+        g.pts.as<float>(), g.stride, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, first_new, first_new, nn, p.seed,
+        max_expand, seeds.as<unsigned long long>());
+    k_apply_seeds<<<blocks_for(static_cast<uint64_t>(nn) * k), kThreads, 0, c.stream>>>(
+        seeds.as<unsigned long long>(), nn, k, first_new, store_of(d.s));
+    count_launch(c, 2);
+    launch_merge(c, g, d.s, nullptr);
+    check_launch(c, "insert seeding");
+    CSB_CUDA(cudaEventRecord(e1, c.stream));
+    // refinement set: new points, then two rings in discovery order, capped
+    uint64_t cap = n;
+    if (p.refine_max_fraction > 0.0 && p.refine_max_fraction < 1.0) cap = static_cast<uint64_t>(p.refine_max_fraction * n);
+    if (p.refine_per_new > 0.0) cap = std::min<uint64_t>(cap, static_cast<uint64_t>(p.refine_per_new * nn));
+    if (cap < nn) cap = nn;
+    DevBuf mark, firstpos, active, flag, off;
+    mark.ensure(n + 16ull);
+    firstpos.ensure(n * 4ull);
+    active.ensure(cap * 4ull + 4);
+    CSB_CUDA(cudaMemsetAsync(mark.p, 0, n, c.stream));
+    k_iota_from<<<blocks_for(nn), kThreads, 0, c.stream>>>(active.as<uint32_t>(), first_new, nn, mark.as<uint8_t>());
+    count_launch(c);
+    uint32_t n_active = nn;
+    const uint32_t r1 = expand_ring(c, g, active.as<uint32_t>(), nn, mark.as<uint8_t>(), firstpos.as<uint32_t>(), flag,
+                                    off, active.as<uint32_t>() + n_active, static_cast<uint32_t>(cap - n_active));
+    n_active += r1;
+    n_active += expand_ring(c, g, active.as<uint32_t>() + nn, r1, mark.as<uint8_t>(), firstpos.as<uint32_t>(), flag, off,
+                            active.as<uint32_t>() + n_active, static_cast<uint32_t>(cap - n_active));
+    uint32_t rounds = 0;
+    const uint64_t upd = d.rounds(active.as<uint32_t>(), n_active, p.refine_iters, p.delta, &rounds);
+    d.finish();
+    CSB_CUDA(cudaEventRecord(e2, c.stream));
+    CSB_CUDA(cudaEventSynchronize(e2));
+    float ms_search = 0.0f, ms_refine = 0.0f;
+    CSB_CUDA(cudaEventElapsedTime(&ms_search, e0, e1));
+    CSB_CUDA(cudaEventElapsedTime(&ms_refine, e1, e2));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    if (st) {
+        st->active = n_active;
+        st->updates = upd;
+        st->rounds = rounds;
+        st->search_ms = ms_search;
+        st->refine_ms = ms_refine;
+    }
 }
 
 }  // namespace csb
@@ -593,6 +876,34 @@ cs_status cs_nndescent(cs_ctx* ctx, const cs_nnd_config* cfg, const float* host_
         if (flags) copy_d2h(*c, flags, g.flags.p, nk);
         copy_d2h(*c, counts, g.counts.p, static_cast<uint64_t>(cfg->n) * 4);
         if (out_updates) *out_updates = upd;
+    });
+}
+
+void cs_insert_defaults(cs_insert_params* p) {
+    if (!p) return;
+    p->sample = 16;
+    p->refine_iters = 5;
+    p->refine_per_new = 2.0;
+    p->refine_max_fraction = 0.25;
+    p->delta = 0.001;
+    p->max_expand = 0;
+    p->seed = 7;
+    p->reselect_bridges = 1;
+}
+
+cs_status cs_insert(cs_graph* gp, const float* rows, uint64_t count, uint32_t row_stride,
+                    const cs_insert_params* params, uint64_t* out_active, uint64_t* out_updates) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(rows != nullptr || count == 0, "cs_insert: null rows");
+        cs_insert_params p;
+        cs_insert_defaults(&p);
+        if (params) p = *params;
+        InsertStats st;
+        knn_insert(*g, rows, count, row_stride, p, &st);
+        if (p.reselect_bridges && count) select_bridges(*g, nullptr, nullptr, nullptr, nullptr);
+        if (out_active) *out_active = st.active;
+        if (out_updates) *out_updates = st.updates;
     });
 }
 
