@@ -155,15 +155,20 @@ cs_status cs_knn_build(cs_graph* g, uint32_t sample, uint32_t iters, double delt
                        uint64_t* out_updates, uint32_t* out_rounds);
 
 /* Parameters of cs_insert; cs_insert_defaults fills the reference's defaults
- * (coresg_cli: sample 16, refine-iters 5, refine-per-new 2.0; IncrementalKnnParams:
- * refine_max_fraction 0.25, search_ef 2k with 4*ef expansions). */
+ * (coresg_cli: sample 16, iters 10, refine-iters 5, context-per-new 2.0,
+ * owned-warm-fraction 0.25, refine-per-new 2.0; IncrementalKnnParams:
+ * refine_max_fraction 0.25; seeding search with 8k expansions). */
 typedef struct {
-    uint32_t sample;            /* smpN of the refinement descent */
-    uint32_t refine_iters;      /* rounds of the restricted descent */
-    double refine_per_new;      /* active-set cap per new point (0: no per-point cap) */
+    uint32_t sample;            /* smpN of both descents */
+    uint32_t instance_iters;    /* rounds over the new points and their context */
+    uint32_t refine_iters;      /* rounds of the restricted refinement */
+    double context_per_new;     /* context nodes per new point in the first descent */
+    double owned_warm_fraction; /* fraction of a new point's seeds it keeps (rest: random batch points) */
+    double refine_per_new;      /* refinement-set cap per new point (0: no per-point cap) */
     double refine_max_fraction; /* active-set cap as a fraction of n (>= 1: none) */
     double delta;               /* stop when a round's updates <= delta * k * |active| */
     uint32_t max_expand;        /* seeding search expansions per point (0: 8k) */
+    uint32_t reverse_cap;       /* reverse neighbours the search expands per node (search_reverse_cap) */
     uint64_t seed;
     int32_t reselect_bridges;   /* 1: re-select the anti-hub bridges afterwards */
 } cs_insert_params;
@@ -177,7 +182,10 @@ void cs_insert_defaults(cs_insert_params* p);
  * points and two rings of their neighbourhoods in discovery order, capped as
  * refinement_set (:927-987); then, optionally, the bridges are re-selected.  The
  * reference splits an insert into instances to bound per-device memory; here the
- * whole graph is resident, so one active set plays every instance.
+ * whole graph is resident, so one active set plays every instance: a descent over the
+ * new points and their context (new points keep owned_warm_fraction of their seeds
+ * and are topped up with random points of the batch, src/incremental_knn.cpp:808-840),
+ * then the restricted refinement.
  * out_active, out_updates may be NULL. */
 cs_status cs_insert(cs_graph* g, const float* rows, uint64_t count, uint32_t row_stride,
                     const cs_insert_params* params, uint64_t* out_active, uint64_t* out_updates);

@@ -169,9 +169,10 @@ class Context:
 
 
 class InsertParams(C.Structure):
-    _fields_ = [("sample", C.c_uint32), ("refine_iters", C.c_uint32), ("refine_per_new", C.c_double),
+    _fields_ = [("sample", C.c_uint32), ("instance_iters", C.c_uint32), ("refine_iters", C.c_uint32),
+                ("context_per_new", C.c_double), ("owned_warm_fraction", C.c_double), ("refine_per_new", C.c_double),
                 ("refine_max_fraction", C.c_double), ("delta", C.c_double), ("max_expand", C.c_uint32),
-                ("seed", C.c_uint64), ("reselect_bridges", C.c_int32)]
+                ("reverse_cap", C.c_uint32), ("seed", C.c_uint64), ("reselect_bridges", C.c_int32)]
 
 
 class MstResult:

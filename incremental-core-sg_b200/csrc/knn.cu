@@ -27,6 +27,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "common.cuh"
 #include "engine.hpp"
 
@@ -171,11 +173,11 @@ __global__ void k_threshold(const float* __restrict__ rank, const uint32_t* __re
 /// Random top-up candidates for short lists (init_random, src/nndescent.cpp:348-377):
 /// `needed + needed/2 + 4` draws per node, in passes of 32 (one per lane), each
 /// followed by a merge.
-__global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_t stride,
+__global__ void k_random_push(const float* __restrict__ pts, uint32_t node_lo, uint32_t node_hi, uint32_t stride,
                               const uint32_t* __restrict__ counts, uint32_t k, uint64_t seed, int pass,
-                              CandStore cand) {
-    const uint32_t p = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    if (p >= n || n < 2) return;
+                              CandStore cand, uint32_t cand_lo, uint32_t cand_span) {
+    const uint32_t p = node_lo + blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (p >= node_hi || cand_span < 2) return;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t c = counts[p];
     if (c >= k) return;
@@ -184,7 +186,7 @@ __global__ void k_random_push(const float* __restrict__ pts, uint32_t n, uint32_
     const uint32_t t = static_cast<uint32_t>(pass) * 32u + lane;
     if (t >= attempts) return;
     const uint64_t h = mix64(seed ^ (0x9E3779B97F4A7C15ull * (p + 1ull)) ^ (0xC2B2AE3D27D4EB4Full * (t + 1ull)));
-    const uint32_t cand_id = static_cast<uint32_t>((h >> 32) % n);
+    const uint32_t cand_id = cand_lo + static_cast<uint32_t>((h >> 32) % cand_span);
     if (cand_id == p) return;
     const float r = l2sqr_ref(pts + static_cast<uint64_t>(p) * stride, pts + static_cast<uint64_t>(cand_id) * stride, stride);
     offer(cand, p, make_key(r, cand_id));
@@ -449,7 +451,9 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
 /// graph only; writes the best k pool keys of query t to seeds[t][*].
 __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const uint32_t* __restrict__ ids,
                          const uint32_t* __restrict__ counts, uint32_t k, uint32_t n_base, uint32_t first_new,
-                         uint32_t count, uint64_t seed, uint32_t max_expand,
+                         uint32_t count, uint64_t seed, uint32_t max_expand, const uint32_t* __restrict__ hints,
+                         uint32_t n_hint, const uint32_t* __restrict__ rev_off,
+                         const unsigned long long* __restrict__ rev_keys, uint32_t rev_cap, uint32_t width,
                          unsigned long long* __restrict__ seeds) {
     extern __shared__ float sq[];
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -468,8 +472,46 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
         unsigned long long ck = make_key(r, e);
         const unsigned same = __match_any_sync(0xFFFFFFFFu, ck);
         if (static_cast<int>(lane) != __ffs(same) - 1) ck = kNoKey;
-        key[0] = key[1] = key[3] = kNoKey;
+        // the two closest of a strided scan of at most 256 hints (the selected
+        // anti-hubs: a coarse index with a quota per component)
+        unsigned long long hk = kNoKey;
+        if (n_hint) {
+            const uint32_t scan = min(n_hint, 256u), step = max(1u, n_hint / scan);
+            const uint32_t off = static_cast<uint32_t>((h & 0xFFFFFFFFull) % n_hint);
+            unsigned long long b0 = kNoKey, b1 = kNoKey;
+            for (uint32_t t2 = lane; t2 < scan; t2 += 32) {
+                const uint32_t e2 = hints[(off + static_cast<uint64_t>(t2) * step) % n_hint];
+                if (e2 >= n_base) continue;
+                const unsigned long long x =
+                    make_key(l2sqr_ref(qrow, pts + static_cast<uint64_t>(e2) * stride, stride), e2);
+                if (x < b0) {
+                    b1 = b0;
+                    b0 = x;
+                } else if (x < b1) {
+                    b1 = x;
+                }
+            }
+            for (int r = 0; r < 2; ++r) {
+                unsigned long long m = b0;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long y = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+                    m = y < m ? y : m;
+                }
+                if (static_cast<uint32_t>(r) == lane) hk = m;
+                if (b0 == m) {  // keys are unique per lane scan; pop the winner
+                    b0 = b1;
+                    b1 = kNoKey;
+                }
+            }
+            // a hint already drawn as a random entry is not entered twice
+            for (int s2 = 0; s2 < 32; ++s2) {
+                const unsigned long long rk = __shfl_sync(0xFFFFFFFFu, ck, s2);
+                if (hk != kNoKey && rk == hk) hk = kNoKey;
+            }
+        }
+        key[0] = key[1] = kNoKey;
         key[2] = ck;
+        key[3] = hk;
         pay[0] = pay[1] = pay[2] = pay[3] = 0;
         warp_bitonic<4>(key, pay);
         key[2] = key[3] = kNoKey;
@@ -491,9 +533,14 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
         }
         const uint32_t c = static_cast<uint32_t>(best);
         const uint32_t cnt = counts[c];
-        for (uint32_t b = 0; b < cnt; b += 32) {
+        // the list, then the first rev_cap reverse neighbours (the undirected graph)
+        const uint32_t r0 = rev_cap ? rev_off[c] : 0u;
+        const uint32_t rc = rev_cap ? min(rev_cap, rev_off[c + 1] - r0) : 0u;
+        for (uint32_t b = 0; b < cnt + rc; b += 32) {
             const uint32_t j = b + lane;
-            const uint32_t nb = j < cnt ? ids[static_cast<uint64_t>(c) * k + j] : kInvalid;
+            uint32_t nb = kInvalid;
+            if (j < cnt) nb = ids[static_cast<uint64_t>(c) * k + j];
+            else if (j < cnt + rc) nb = static_cast<uint32_t>(rev_keys[r0 + (j - cnt)]);
             bool ok = nb < n_base;
             unsigned long long ck = kNoKey;
             if (ok) ck = make_key(l2sqr_ref(qrow, pts + static_cast<uint64_t>(nb) * stride, stride), nb);
@@ -504,6 +551,10 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
                     if (pk != kNoKey && static_cast<uint32_t>(pk) == nb) ok = false;
                 }
             }
+            {  // forward and reverse entries can name the same node
+                const unsigned same = __match_any_sync(0xFFFFFFFFu, nb);
+                if (static_cast<int>(lane) != __ffs(same) - 1) ok = false;
+            }
             key[2] = ok ? ck : kNoKey;
             pay[2] = 0;
             key[3] = kNoKey;
@@ -513,7 +564,7 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
             key[2] = key[3] = kNoKey;
         }
     }
-    for (uint32_t e = lane; e < k; e += 32) {
+    for (uint32_t e = lane; e < width; e += 32) {
         const int i = static_cast<int>(e / 32);
         // element e = i*32 + lane of the sorted pool
         unsigned long long x = kNoKey;
@@ -521,33 +572,48 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
         for (int ii = 0; ii < 2; ++ii) {
             if (ii == i) x = key[ii];
         }
-        seeds[static_cast<uint64_t>(t) * k + e] = x;
+        seeds[static_cast<uint64_t>(t) * width + e] = x;
     }
 }
 
 /// Apply the seeds symmetrically: q <- s and s <- q (src/incremental_knn.cpp:1195-1200).
-__global__ void k_apply_seeds(const unsigned long long* __restrict__ seeds, uint32_t count, uint32_t k,
+__global__ void k_apply_seeds(const unsigned long long* __restrict__ seeds, uint32_t count, uint32_t width,
                               uint32_t first_new, CandStore cand) {
     const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (x >= static_cast<uint64_t>(count) * k) return;
+    if (x >= static_cast<uint64_t>(count) * width) return;
     const unsigned long long key = seeds[x];
     if (key == kNoKey) return;
-    const uint32_t q = first_new + static_cast<uint32_t>(x / k);
+    const uint32_t q = first_new + static_cast<uint32_t>(x / width);
     const uint32_t s = static_cast<uint32_t>(key);
     const float r = __uint_as_float(static_cast<uint32_t>(key >> 32));
     offer(cand, q, make_key(r, s));
     offer(cand, s, make_key(r, q));
 }
 
-/// One ring of refinement_set (src/incremental_knn.cpp:927-987) in discovery order:
-/// the sequence is (src[t], j) for the list entries of the source nodes in order;
-/// a node joins the ring at its first position in the sequence if unmarked.
+/// Position x of a ring sequence: source-major (x = i*k + j, discovery order) or
+/// rank-major (x = j*ns + i: every source's nearest entry before any second one).
+__device__ __forceinline__ void ring_pos(uint64_t x, uint32_t ns, uint32_t k, bool rank_major, uint32_t* i,
+                                         uint32_t* j) {
+    if (rank_major) {
+        *i = static_cast<uint32_t>(x % ns);
+        *j = static_cast<uint32_t>(x / ns);
+    } else {
+        *i = static_cast<uint32_t>(x / k);
+        *j = static_cast<uint32_t>(x % k);
+    }
+}
+
+/// One ring of refinement_set (src/incremental_knn.cpp:927-987): the sequence is
+/// (src[i], j) over the list entries of the source nodes; a node joins the ring at its
+/// first position in the sequence if unmarked.
 __global__ void k_ring_first(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids,
                              const uint32_t* __restrict__ counts, uint32_t k, uint32_t n,
-                             const uint8_t* __restrict__ mark, uint32_t* __restrict__ firstpos) {
+                             const uint8_t* __restrict__ mark, uint32_t* __restrict__ firstpos, bool rank_major) {
     const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (x >= static_cast<uint64_t>(ns) * k) return;
-    const uint32_t v = src[x / k], j = static_cast<uint32_t>(x % k);
+    uint32_t i, j;
+    ring_pos(x, ns, k, rank_major, &i, &j);
+    const uint32_t v = src[i];
     if (j >= counts[v]) return;
     const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
     if (q < n && !mark[q]) atomicMin(firstpos + q, static_cast<uint32_t>(x));
@@ -556,10 +622,12 @@ __global__ void k_ring_first(const uint32_t* __restrict__ src, uint32_t ns, cons
 __global__ void k_ring_flag(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids,
                             const uint32_t* __restrict__ counts, uint32_t k, uint32_t n,
                             const uint8_t* __restrict__ mark, const uint32_t* __restrict__ firstpos,
-                            uint32_t* __restrict__ flag) {
+                            uint32_t* __restrict__ flag, bool rank_major) {
     const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (x >= static_cast<uint64_t>(ns) * k) return;
-    const uint32_t v = src[x / k], j = static_cast<uint32_t>(x % k);
+    uint32_t i, j;
+    ring_pos(x, ns, k, rank_major, &i, &j);
+    const uint32_t v = src[i];
     uint32_t f = 0;
     if (j < counts[v]) {
         const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
@@ -570,12 +638,14 @@ __global__ void k_ring_flag(const uint32_t* __restrict__ src, uint32_t ns, const
 
 __global__ void k_ring_emit(const uint32_t* __restrict__ src, uint32_t ns, const uint32_t* __restrict__ ids, uint32_t k,
                             const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off, uint32_t limit,
-                            uint8_t* __restrict__ mark, uint32_t* __restrict__ out) {
+                            uint8_t* __restrict__ mark, uint32_t* __restrict__ out, bool rank_major) {
     const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (x >= static_cast<uint64_t>(ns) * k || !flag[x]) return;
     const uint32_t pos = off[x];
     if (pos >= limit) return;
-    const uint32_t q = ids[static_cast<uint64_t>(src[x / k]) * k + x % k];
+    uint32_t i, j;
+    ring_pos(x, ns, k, rank_major, &i, &j);
+    const uint32_t q = ids[static_cast<uint64_t>(src[i]) * k + j];
     mark[q] = 1;
     out[pos] = q;
 }
@@ -585,6 +655,47 @@ __global__ void k_iota_from(uint32_t* __restrict__ out, uint32_t first, uint32_t
     if (t >= count) return;
     out[t] = first + t;
     mark[first + t] = 1;
+}
+
+/// Keep the first `keep` entries of nodes [lo, hi) (owned_warm_fraction,
+/// src/incremental_knn.cpp:808-840): the freed slots let the random fill put other
+/// new points of the batch there.
+__global__ void k_truncate(uint32_t* __restrict__ ids, float* __restrict__ rank, uint8_t* __restrict__ flags,
+                           uint32_t* __restrict__ counts, float* __restrict__ thr, uint32_t k, uint32_t lo,
+                           uint32_t hi, uint32_t keep) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t span = static_cast<uint64_t>(hi - lo) * k;
+    if (x >= span) return;
+    const uint32_t v = lo + static_cast<uint32_t>(x / k), j = static_cast<uint32_t>(x % k);
+    if (j >= keep) {
+        ids[static_cast<uint64_t>(v) * k + j] = kInvalid;
+        rank[static_cast<uint64_t>(v) * k + j] = __int_as_float(0x7f800000);
+        flags[static_cast<uint64_t>(v) * k + j] = 0;
+    }
+    if (j == 0) {
+        counts[v] = min(counts[v], keep);
+        thr[v] = __int_as_float(0x7f800000);
+    }
+}
+
+/// Reverse adjacency of the base graph as sorted (target << 32 | source) keys; the
+/// sort makes each node's reverse list ascending by source, so a capped prefix is
+/// the same on every run (the reference reads its ReverseNeighbours table,
+/// src/incremental_knn.cpp:185-189).
+__global__ void k_rev_keys(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t k,
+                           uint32_t n_base, unsigned long long* __restrict__ keys, uint32_t* __restrict__ rdeg) {
+    const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (x >= static_cast<uint64_t>(n_base) * k) return;
+    const uint32_t v = static_cast<uint32_t>(x / k), j = static_cast<uint32_t>(x % k);
+    unsigned long long key = ~0ull;
+    if (j < counts[v]) {
+        const uint32_t t = ids[x];
+        if (t < n_base) {
+            key = (static_cast<unsigned long long>(t) << 32) | v;
+            atomicAdd(rdeg + t, 1u);
+        }
+    }
+    keys[x] = key;
 }
 
 struct KnnScratch {
@@ -670,13 +781,17 @@ struct Descent {
         check_launch(c, "NN-Descent setup");
     }
 
-    /// init_random: top every short list up with random candidates.
-    void random_fill(uint64_t seed) {
-        const unsigned gw = static_cast<unsigned>((n + kWarps - 1) / kWarps);
+    /// init_random: top the short lists of nodes [lo, hi) up with random candidates
+    /// drawn from [cand_lo, cand_lo + cand_span) (all nodes by default).
+    void random_fill(uint64_t seed, uint32_t lo = 0, uint32_t hi = 0xFFFFFFFFu, uint32_t cand_lo = 0,
+                     uint32_t cand_span = 0) {
+        if (hi > n) hi = n;
+        if (!cand_span) cand_span = n;
+        const unsigned gw = static_cast<unsigned>(std::max<uint32_t>(1, (hi - lo + kWarps - 1) / kWarps));
         const uint32_t max_attempts = k + k / 2 + 4;
         for (int pass = 0; pass * 32u < max_attempts; ++pass) {
-            k_random_push<<<gw, kThreads, 0, c.stream>>>(g.pts.as<float>(), n, g.stride, g.counts.as<uint32_t>(), k, seed,
-                                                          pass, store_of(s));
+            k_random_push<<<gw, kThreads, 0, c.stream>>>(g.pts.as<float>(), lo, hi, g.stride, g.counts.as<uint32_t>(), k,
+                                                          seed, pass, store_of(s), cand_lo, cand_span);
             count_launch(c);
             launch_merge(c, g, s, nullptr);
         }
@@ -744,7 +859,7 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
 /// One ring of refinement_set appended to `out` at `at` (at most `limit` nodes);
 /// returns the ring's size.
 uint32_t expand_ring(Ctx& c, Graph& g, const uint32_t* src, uint32_t ns, uint8_t* mark, uint32_t* firstpos,
-                     DevBuf& flag, DevBuf& off, uint32_t* out, uint32_t limit) {
+                     DevBuf& flag, DevBuf& off, uint32_t* out, uint32_t limit, bool rank_major) {
     if (ns == 0 || limit == 0) return 0;
     const uint32_t n = static_cast<uint32_t>(g.n), k = g.k;
     const uint64_t seq = static_cast<uint64_t>(ns) * k;
@@ -753,16 +868,16 @@ uint32_t expand_ring(Ctx& c, Graph& g, const uint32_t* src, uint32_t ns, uint8_t
     off.ensure(seq * 4 + 8);
     CSB_CUDA(cudaMemsetAsync(firstpos, 0xFF, n * 4ull, c.stream));
     k_ring_first<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, n,
-                                                            mark, firstpos);
+                                                            mark, firstpos, rank_major);
     k_ring_flag<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, n,
-                                                           mark, firstpos, flag.as<uint32_t>());
+                                                           mark, firstpos, flag.as<uint32_t>(), rank_major);
     count_launch(c, 2);
     scan_u32(c, flag.as<uint32_t>(), off.as<uint32_t>(), seq);
     uint32_t total = 0;
     CSB_CUDA(cudaMemcpyAsync(&total, off.as<uint32_t>() + seq, 4, cudaMemcpyDeviceToHost, c.stream));
     CSB_CUDA(cudaStreamSynchronize(c.stream));
     k_ring_emit<<<blocks_for(seq), kThreads, 0, c.stream>>>(src, ns, g.ids.as<uint32_t>(), k, flag.as<uint32_t>(),
-                                                           off.as<uint32_t>(), limit, mark, out);
+                                                           off.as<uint32_t>(), limit, mark, out, rank_major);
     count_launch(c);
     check_launch(c, "refinement ring");
     return std::min(total, limit);
@@ -782,40 +897,112 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     CSB_CUDA(cudaEventCreate(&e2));
     Descent d(g, p.sample);
     CSB_CUDA(cudaEventRecord(e0, c.stream));
-    // seeding search over the base graph, then the seeds both ways
-    DevBuf seeds;
-    seeds.ensure(static_cast<uint64_t>(nn) * k * 8);
+    // seeding search over the base graph (ef = 2k results, at most the 64-entry
+    // pool; the selected anti-hubs as extra entry points), then the seeds both ways
+    const uint32_t width = std::min<uint32_t>(2 * k, 64);
+    DevBuf seeds, hints;
+    seeds.ensure(static_cast<uint64_t>(nn) * width * 8);
+    const uint32_t n_hint = static_cast<uint32_t>(g.selected.size());
+    if (n_hint) {
+        hints.ensure(n_hint * 4ull);
+        copy_h2d(c, hints.p, g.selected.data(), n_hint * 4ull);
+    }
+    DevBuf rev_keys, rev_alt, rev_deg, rev_off, sort_tmp;
+    if (p.reverse_cap) {
+        const uint64_t nk = static_cast<uint64_t>(first_new) * k;
+        CSB_REQUIRE(nk < 0x7FFFFFFFull, "cs_insert: base graph too large for the reverse index");
+        rev_keys.ensure(nk * 8 + 8);
+        rev_alt.ensure(nk * 8 + 8);
+        rev_deg.ensure(first_new * 4ull + 8);
+        rev_off.ensure(first_new * 4ull + 8);
+        CSB_CUDA(cudaMemsetAsync(rev_deg.p, 0, first_new * 4ull + 8, c.stream));
+        k_rev_keys<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k,
+                                                               first_new, rev_keys.as<unsigned long long>(),
+                                                               rev_deg.as<uint32_t>());
+        count_launch(c);
+        // targets fit below bit end_bit; a valid key's source is < 2^32 - 1, so the
+        // invalid key ~0 still sorts after every valid one over bits [0, end_bit)
+        int end_bit = 33;
+        while (end_bit < 64 && (1ull << (end_bit - 32)) <= first_new) ++end_bit;
+        cub::DoubleBuffer<unsigned long long> db(rev_keys.as<unsigned long long>(), rev_alt.as<unsigned long long>());
+        size_t tmp_bytes = 0;
+        CSB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(nk), 0, end_bit, c.stream));
+        sort_tmp.ensure(tmp_bytes + 16);
+        CSB_CUDA(cub::DeviceRadixSort::SortKeys(sort_tmp.p, tmp_bytes, db, static_cast<int>(nk), 0, end_bit, c.stream));
+        count_launch(c, static_cast<uint64_t>((end_bit + 7) / 8) + 1);  // histogram + one per digit
+        if (db.Current() != rev_keys.as<unsigned long long>()) std::swap(rev_keys.p, rev_alt.p);
+        scan_u32(c, rev_deg.as<uint32_t>(), rev_off.as<uint32_t>(), first_new);
+        check_launch(c, "insert reverse index");
+    }
     const uint32_t max_expand = p.max_expand ? p.max_expand : 8 * k;
     const size_t qsmem = static_cast<size_t>(kWarps) * g.stride * 4;
     k_search<<<(nn + kWarps - 1) / kWarps, kThreads, qsmem, c.stream>>>(
         g.pts.as<float>(), g.stride, g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k, first_new, first_new, nn, p.seed,
-        max_expand, seeds.as<unsigned long long>());
-    k_apply_seeds<<<blocks_for(static_cast<uint64_t>(nn) * k), kThreads, 0, c.stream>>>(
-        seeds.as<unsigned long long>(), nn, k, first_new, store_of(d.s));
+        max_expand, hints.as<uint32_t>(), n_hint, rev_off.as<uint32_t>(), rev_keys.as<unsigned long long>(),
+        p.reverse_cap, width, seeds.as<unsigned long long>());
+    k_apply_seeds<<<blocks_for(static_cast<uint64_t>(nn) * width), kThreads, 0, c.stream>>>(
+        seeds.as<unsigned long long>(), nn, width, first_new, store_of(d.s));
     count_launch(c, 2);
     launch_merge(c, g, d.s, nullptr);
     check_launch(c, "insert seeding");
     CSB_CUDA(cudaEventRecord(e1, c.stream));
-    // refinement set: new points, then two rings in discovery order, capped
-    uint64_t cap = n;
-    if (p.refine_max_fraction > 0.0 && p.refine_max_fraction < 1.0) cap = static_cast<uint64_t>(p.refine_max_fraction * n);
-    if (p.refine_per_new > 0.0) cap = std::min<uint64_t>(cap, static_cast<uint64_t>(p.refine_per_new * nn));
-    if (cap < nn) cap = nn;
     DevBuf mark, firstpos, active, flag, off;
     mark.ensure(n + 16ull);
     firstpos.ensure(n * 4ull);
-    active.ensure(cap * 4ull + 4);
-    CSB_CUDA(cudaMemsetAsync(mark.p, 0, n, c.stream));
-    k_iota_from<<<blocks_for(nn), kThreads, 0, c.stream>>>(active.as<uint32_t>(), first_new, nn, mark.as<uint8_t>());
-    count_launch(c);
-    uint32_t n_active = nn;
-    const uint32_t r1 = expand_ring(c, g, active.as<uint32_t>(), nn, mark.as<uint8_t>(), firstpos.as<uint32_t>(), flag,
-                                    off, active.as<uint32_t>() + n_active, static_cast<uint32_t>(cap - n_active));
-    n_active += r1;
-    n_active += expand_ring(c, g, active.as<uint32_t>() + nn, r1, mark.as<uint8_t>(), firstpos.as<uint32_t>(), flag, off,
-                            active.as<uint32_t>() + n_active, static_cast<uint32_t>(cap - n_active));
-    uint32_t rounds = 0;
-    const uint64_t upd = d.rounds(active.as<uint32_t>(), n_active, p.refine_iters, p.delta, &rounds);
+    active.ensure(static_cast<uint64_t>(n) * 4 + 4);
+    // the active set of a pass: the new points, then two rings, capped.  For the
+    // instance (make_anchored_instances, src/incremental_knn.cpp:652-705) ring one is
+    // the seeds rank by rank and ring two their neighbours; for the refinement
+    // (refinement_set) both rings are in discovery order.
+    auto active_set = [&](uint64_t cap, bool seeds_by_rank) -> uint32_t {
+        if (cap < nn) cap = nn;
+        if (cap > n) cap = n;
+        CSB_CUDA(cudaMemsetAsync(mark.p, 0, n, c.stream));
+        k_iota_from<<<blocks_for(nn), kThreads, 0, c.stream>>>(active.as<uint32_t>(), first_new, nn, mark.as<uint8_t>());
+        count_launch(c);
+        uint32_t na = nn;
+        const uint32_t r1 = expand_ring(c, g, active.as<uint32_t>(), nn, mark.as<uint8_t>(), firstpos.as<uint32_t>(),
+                                        flag, off, active.as<uint32_t>() + na, static_cast<uint32_t>(cap - na),
+                                        seeds_by_rank);
+        na += r1;
+        na += expand_ring(c, g, active.as<uint32_t>() + nn, r1, mark.as<uint8_t>(), firstpos.as<uint32_t>(), flag, off,
+                          active.as<uint32_t>() + na, static_cast<uint32_t>(cap - na), false);
+        return na;
+    };
+    // the instance: new points plus their context (context_per_new per point), taken
+    // while the new points' lists still hold every seed
+    uint32_t n_active = active_set(static_cast<uint64_t>((1.0 + p.context_per_new) * nn), true);
+    // owned nodes keep the head of their seed lists; the rest is filled with random
+    // points of the batch, so the batch's own neighbourhoods get built
+    const uint32_t keep = p.owned_warm_fraction >= 1.0 ? k : static_cast<uint32_t>(p.owned_warm_fraction * k);
+    if (keep < k) {
+        k_truncate<<<blocks_for(static_cast<uint64_t>(nn) * k), kThreads, 0, c.stream>>>(
+            g.ids.as<uint32_t>(), g.dists.as<float>(), g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), d.s.thr.as<float>(),
+            k, first_new, n, keep);
+        count_launch(c);
+        d.random_fill(p.seed ^ 0x5851F42D4C957F2Dull, first_new, n, first_new, nn);
+    }
+    uint32_t rounds = 0, r2 = 0;
+    uint64_t upd = d.rounds(active.as<uint32_t>(), n_active, p.instance_iters, p.delta, &rounds);
+    // merge_job: the truncation was local to the instance, the global lists keep
+    // every seed -- offer them again next to what the instance found
+    if (keep < k) {
+        k_apply_seeds<<<blocks_for(static_cast<uint64_t>(nn) * width), kThreads, 0, c.stream>>>(
+            seeds.as<unsigned long long>(), nn, width, first_new, store_of(d.s));
+        count_launch(c);
+        launch_merge(c, g, d.s, nullptr);
+        check_launch(c, "insert seed merge");
+    }
+    // the restricted refinement (refine_per_new, refine_max_fraction)
+    uint64_t cap = n;
+    if (p.refine_max_fraction > 0.0 && p.refine_max_fraction < 1.0) cap = static_cast<uint64_t>(p.refine_max_fraction * n);
+    if (p.refine_per_new > 0.0) cap = std::min<uint64_t>(cap, static_cast<uint64_t>(p.refine_per_new * nn));
+    if (p.refine_iters) {
+        const uint32_t n_ref = active_set(cap, false);
+        upd += d.rounds(active.as<uint32_t>(), n_ref, p.refine_iters, p.delta, &r2);
+        n_active = std::max(n_active, n_ref);
+    }
+    rounds += r2;
     d.finish();
     CSB_CUDA(cudaEventRecord(e2, c.stream));
     CSB_CUDA(cudaEventSynchronize(e2));
@@ -882,11 +1069,15 @@ cs_status cs_nndescent(cs_ctx* ctx, const cs_nnd_config* cfg, const float* host_
 void cs_insert_defaults(cs_insert_params* p) {
     if (!p) return;
     p->sample = 16;
+    p->instance_iters = 10;
     p->refine_iters = 5;
+    p->context_per_new = 2.0;
+    p->owned_warm_fraction = 0.25;
     p->refine_per_new = 2.0;
     p->refine_max_fraction = 0.25;
     p->delta = 0.001;
     p->max_expand = 0;
+    p->reverse_cap = 16;
     p->seed = 7;
     p->reselect_bridges = 1;
 }
