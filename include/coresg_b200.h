@@ -255,6 +255,88 @@ cs_status cs_set_sweep_shape(cs_graph* g, uint32_t flatten_div, uint32_t block_t
 cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_flatten,
                             uint32_t* out_block);
 
+/* ---- serving loop (no counterpart in the reference) -------------------------- */
+
+/* A device-resident request loop over one cs_graph: extract(mpts) queries,
+ * epsilon-cut label queries and insert batches are submitted from any host thread
+ * and served in arrival order.  Consecutive queries are batched as they arrive:
+ * every batch is one 32-lane graph-captured sweep over the distinct mpts it holds
+ * (a query that arrives while a batch is on the GPU joins the next one), its
+ * results are copied into device result slots in stream order, and a completion
+ * thread copies the slots into the callers' host buffers on a second stream while
+ * the next sweep runs.  An insert is a barrier: queries before it see the graph
+ * without its rows, queries after it see them (CoreSG::insert, then the bridges are
+ * re-selected).  Admission is by free HBM: a result slot is allocated only while
+ * cudaMemGetInfo leaves `reserve_bytes` free, otherwise the batch is cut short and
+ * waits for slots in flight; an insert whose growth does not fit fails with
+ * CS_ERR_OOM.  The graph must not be used through other entry points while a server
+ * runs on it.  Results equal cs_extract on the graph state the request saw; an
+ * epsilon-cut equals dbscan_labels_from_mst (src/eval.cpp:230-239) on that tree:
+ * union of the tree edges with double(w) <= eps, dense labels by smallest node. */
+typedef struct cs_server cs_server;
+
+enum { CS_REQ_EXTRACT = 0, CS_REQ_EPS_LABELS = 1, CS_REQ_INSERT = 2 };
+
+typedef struct {
+    uint32_t max_batch;       /* distinct mpts per sweep, 1..32 (0: 32) */
+    uint32_t max_slots;       /* result slots in flight (0: 64) */
+    uint64_t reserve_bytes;   /* HBM left free by admission (0: 2 GiB) */
+    cs_insert_params insert;  /* parameters of every insert (cs_insert_defaults if
+                                 sample == 0) */
+} cs_server_config;
+
+typedef struct {
+    int32_t kind;              /* CS_REQ_* */
+    uint32_t mpts;             /* extract / epsilon-cut: 0..k_max (0 == 1) */
+    double eps;                /* epsilon-cut threshold on the MRD merge heights */
+    const float* rows;         /* insert: count rows of row_stride floats (copied at
+                                  submit, the buffer is free on return) */
+    uint64_t count;
+    uint32_t row_stride;
+    cs_edge* out_edges;        /* extract: the tree (optional); holds out_edges_cap edges */
+    uint64_t out_edges_cap;
+    uint32_t* out_labels;      /* extract: MST component labels (optional);
+                                  epsilon-cut: the cut's labels (required) */
+    uint64_t out_labels_cap;
+} cs_request;
+
+typedef struct {
+    int32_t status;            /* the request's own status */
+    uint32_t ncomp;            /* components of the MST / of the cut */
+    uint64_t nedges;           /* tree edges (extract) */
+    uint64_t n;                /* graph size the request saw */
+    double weight;             /* exact tree weight (extract) */
+    double queue_ms;           /* submit -> dispatched to the GPU */
+    double latency_ms;         /* submit -> result in the caller's buffers */
+    uint64_t batch;            /* sweep batch that served it (0: insert) */
+    char error[160];           /* message when status != CS_OK */
+} cs_result;
+
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint64_t batches;          /* sweeps run */
+    uint64_t queries;          /* extract + epsilon-cut requests served */
+    uint64_t inserts, inserted_rows;
+    uint64_t slots, slot_bytes;  /* result slots allocated, bytes each */
+    uint32_t max_batch_seen;   /* most requests served by one sweep */
+    double sweep_ms;           /* device time of all sweeps */
+    double insert_ms;          /* host time of all inserts */
+} cs_server_stats;
+
+cs_status cs_server_create(cs_graph* g, const cs_server_config* cfg, cs_server** out);
+/* Finishes every submitted request, then stops the threads and frees the slots. */
+void cs_server_destroy(cs_server* s);
+/* Queue a request; *out_ticket identifies it for cs_server_wait. */
+cs_status cs_server_submit(cs_server* s, const cs_request* req, uint64_t* out_ticket);
+/* Wait up to timeout_ms (UINT32_MAX: forever) for a ticket; on completion fills
+ * *out and releases the ticket.  CS_ERR_TIMEOUT when it is still pending. */
+cs_status cs_server_wait(cs_server* s, uint64_t ticket, uint32_t timeout_ms, cs_result* out);
+cs_status cs_server_stats_get(cs_server* s, cs_server_stats* out);
+/* Page-locked host memory for request buffers (the completion copies run
+ * asynchronously only into pinned memory). */
+void* cs_host_alloc(size_t bytes);
+void cs_host_free(void* p);
+
 /* ---- allocation-free MST (no counterpart in the reference) ------------------- */
 
 /* MST of a caller-provided edge list that allocates nothing, for callers that

@@ -75,6 +75,13 @@ _SIGS = {
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
     "cs_mst_noalloc": (_i32, [_p, _p, _p, _u64, _u32, _p, _p, _p, _p, _p, _p]),
+    "cs_server_create": (_i32, [_p, _p, _pp]),
+    "cs_server_destroy": (None, [_p]),
+    "cs_server_submit": (_i32, [_p, _p, _p]),
+    "cs_server_wait": (_i32, [_p, _u64, _u32, _p]),
+    "cs_server_stats_get": (_i32, [_p, _p]),
+    "cs_host_alloc": (_p, [_sz]),
+    "cs_host_free": (None, [_p]),
 }
 
 _lib = None

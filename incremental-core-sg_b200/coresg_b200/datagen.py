@@ -84,3 +84,17 @@ def pad_rows(x: np.ndarray) -> np.ndarray:
     out = np.zeros((n, stride), dtype=np.float32)
     out[:, :d] = x
     return out
+
+
+def workload_centres(w: dict) -> np.ndarray:
+    """The cluster centres of a named workload's mixture (the first draw of its
+    stream, as gaussian_mixture makes them)."""
+    return np.random.default_rng(w["seed"]).uniform(0.0, 10.0, size=(w["clusters"], w["dim"]))
+
+
+def insert_batch(w: dict, size: int, seed: int, new_clusters: int = 0) -> np.ndarray:
+    """An insertion batch for workload `w`: drawn from its existing clusters, or
+    from `new_clusters` fresh centres uniform in [0, 10]^d."""
+    if new_clusters:
+        return gaussian_mixture(size, w["dim"], new_clusters, w["sigma"], 0.0, seed)
+    return gaussian_mixture(size, w["dim"], w["clusters"], w["sigma"], 0.0, seed, centres=workload_centres(w))

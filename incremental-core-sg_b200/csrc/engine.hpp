@@ -155,6 +155,15 @@ void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_la
 void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms);
 void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
 void sweep_free(SweepPlan* p);
+/// Device outputs of MST `index` of the last sweep, valid until the next sweep.
+struct SweepOut {
+    const cs_edge* edges = nullptr;             // [cap] tree edges, ascending edge index
+    const uint32_t* labels = nullptr;           // [n] (null when the sweep ran without labels)
+    const unsigned long long* count = nullptr;  // tree edges
+    const unsigned long long* bins = nullptr;   // [256] exact-sum bins of the tree weights
+    uint64_t cap = 0, n = 0;
+};
+SweepOut sweep_outputs(Graph& g, uint32_t index);
 double exact_sum_from_bins(const uint64_t* bins256);
 /// Dense labels (numbered by smallest node) of K union-find forests parent_all[K][n]
 /// whose roots are their sets' smallest nodes; component counts -> ncomp[K].

@@ -801,6 +801,25 @@ void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_lab
     if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n, static_cast<uint64_t>(p->n) * 4);
 }
 
+SweepOut sweep_outputs(Graph& g, uint32_t index) {
+    if (!g.plan) fail(CS_ERR_STATE, "sweep: no sweep has run");
+    if (index >= g.sweep_K) fail(CS_ERR_INVALID, "sweep: index out of range");
+    SweepPlan* p = g.plan;
+    uint32_t j = index;
+    while (j >= p->K) {
+        j -= p->K;
+        p = p->next;
+    }
+    SweepOut o;
+    o.n = p->n;
+    o.cap = p->n ? p->n - 1 : 0;
+    o.edges = p->out.as<cs_edge>() + j * o.cap;
+    o.labels = p->labels ? p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n : nullptr;
+    o.count = p->counts.as<unsigned long long>() + j;
+    o.bins = p->bins.as<unsigned long long>() + static_cast<uint64_t>(j) * 256;
+    return o;
+}
+
 }  // namespace csb
 
 // ============================================================================

@@ -36,3 +36,32 @@ def test_no_gpu_is_reported_not_crashed():
 def test_null_context_is_invalid():
     st = cs.lib().cs_graph_create(None, 8, 8, 0, C.byref(C.c_void_p()))
     assert st == cs.CS_ERR_INVALID
+
+
+def test_server_structs_match_the_header_layout():
+    """ctypes mirrors of the serving structs have the C layout of coresg_b200.h
+    (natural alignment on x86-64)."""
+    import ctypes as C
+
+    from coresg_b200.serving import Request, Result, ServerConfig, Stats
+
+    assert C.sizeof(Request) == 72 and Request.eps.offset == 8 and Request.out_labels_cap.offset == 64
+    assert C.sizeof(Result) == 216 and Result.weight.offset == 24 and Result.error.offset == 56
+    assert C.sizeof(ServerConfig) == 96 and ServerConfig.insert.offset == 16
+    assert C.sizeof(Stats) == 96 and Stats.sweep_ms.offset == 80
+
+
+def test_request_stream_is_seeded_and_shaped():
+    from coresg_b200.serving import CS_REQ_EPS_LABELS, CS_REQ_INSERT, request_stream
+
+    a = request_stream(20.0, 200.0, 32, seed=9)
+    b = request_stream(20.0, 200.0, 32, seed=9)
+    assert a == b
+    assert 3600 < len(a) < 4400  # Poisson(4000)
+    ins = [x for x in a if x.kind == CS_REQ_INSERT]
+    cuts = [x for x in a if x.kind == CS_REQ_EPS_LABELS]
+    assert 0.07 < len(ins) / len(a) < 0.13
+    assert all(1_000 <= x.size <= 100_000 for x in ins)
+    assert all(1 <= x.mpts <= 32 for x in a if x.kind != CS_REQ_INSERT)
+    assert 0.18 < len(cuts) / (len(a) - len(ins)) < 0.32
+    assert all(a[i].t < a[i + 1].t for i in range(len(a) - 1))
