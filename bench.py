@@ -186,6 +186,99 @@ def cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges):
         return None
 
 
+def run_serving(cs, ctx, args):
+    """The serving workload: a resident CORE-SG of the serve workload, Poisson
+    arrivals (extract(mpts ~ U{1..k_max}), a quarter of them epsilon-cuts at a random
+    merge-height quantile, and 10% insert batches of log-uniform size) submitted on
+    schedule from one host thread; a second thread waits on the tickets.  Latency =
+    (submit - scheduled arrival) + the server's submit-to-result time."""
+    import queue
+    import threading
+
+    from coresg_b200.datagen import insert_batch, workload
+    from coresg_b200.serving import CS_REQ_EPS_LABELS, CS_REQ_INSERT, Pinned, Server, percentile, request_stream
+
+    pts, w = workload(args.serve_workload)
+    n0, K = w["n"], w["k_max"]
+    g = cs.CoreSG(ctx, w["dim"], K)
+    t0 = time.perf_counter()
+    g.build(pts, sample=16, iters=10, delta=0.001, seed=43)
+    build_s = time.perf_counter() - t0
+    del pts
+    stream = request_stream(args.serve_seconds, args.serve_rate, K, seed=w["seed"])
+    # epsilon values: quantiles of each mpts tree's merge heights on the built graph
+    mp = list(range(1, K + 1))
+    g.sweep_device(mp)
+    grid = np.linspace(0.0, 1.0, 101)
+    qs = {m: np.quantile(g.sweep_fetch(m - 1, labels=False).edges["w"][::16], grid) for m in mp}
+    batches = {i: insert_batch(w, a.size, a.seed) for i, a in enumerate(stream) if a.kind == CS_REQ_INSERT}
+    n_max = n0 + sum(len(b) for b in batches.values())
+    pool = [Pinned((3 * n_max,), np.uint32) for _ in range(args.serve_buffers)]
+    free = queue.Queue()
+    for i in range(len(pool)):
+        free.put(i)
+    srv = Server(g, max_batch=32, max_slots=64, inserts_first=bool(args.serve_inserts_first))
+    done, sent = queue.Queue(), queue.Queue()
+
+    def waiter():
+        while True:
+            item = sent.get()
+            if item is None:
+                return
+            ticket, arr, buf, t_sub = item
+            r = srv.wait(ticket)
+            if buf is not None:
+                free.put(buf)
+            done.put((arr, (t_sub - arr.t) * 1000.0 + r["latency_ms"], r, time.perf_counter()))
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t_start = time.perf_counter()
+    for i, a in enumerate(stream):
+        delay = t_start + a.t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        buf = None
+        if a.kind == CS_REQ_INSERT:
+            ticket = srv.insert(batches.pop(i))
+        else:
+            buf = free.get()
+            arr = pool[buf].array
+            if a.kind == CS_REQ_EPS_LABELS:
+                eps = float(np.interp(a.quantile, grid, qs[a.mpts]))
+                ticket = srv.cut(a.mpts, eps, arr[:n_max])
+            else:
+                ticket = srv.extract(a.mpts, arr.view(cs.EDGE_DTYPE))
+        sent.put((ticket, a, buf, time.perf_counter() - t_start))
+    sent.put(None)
+    th.join()
+    st = srv.stats()
+    srv.close()
+    qlat, ilat, failed, t_last = [], [], 0, t_start
+    while not done.empty():
+        arr, ms, r, t_done = done.get()
+        failed += r["status"] != 0
+        (ilat if arr.kind == CS_REQ_INSERT else qlat).append(ms)
+        t_last = max(t_last, t_done)
+    for p_ in pool:
+        p_.free()
+    drain = t_last - t_start
+    return {
+        "workload": args.serve_workload, "n_start": n0, "n_end": int(g.n), "k_max": K, "build_s": build_s,
+        "window_s": args.serve_seconds, "rate_per_s": args.serve_rate,
+        "consistency": "inserts_first" if args.serve_inserts_first else "arrival_order",
+        "requests": len(stream), "queries": len(qlat), "inserts": len(ilat), "failed": failed,
+        "p50_query_ms": percentile(qlat, 50), "p99_query_ms": percentile(qlat, 99),
+        "p50_insert_ms": percentile(ilat, 50), "p99_insert_ms": percentile(ilat, 99),
+        "p50_ms": percentile(qlat + ilat, 50), "p99_ms": percentile(qlat + ilat, 99),
+        "msts_per_s": len(qlat) / drain if drain > 0 else None, "drain_s": drain,
+        "sweeps": st["batches"], "mean_batch": (st["queries"] / st["batches"]) if st["batches"] else None,
+        "max_batch": st["max_batch_seen"], "insert_batches": st["insert_batches"],
+        "inserted_rows": st["inserted_rows"], "sweep_ms_total": st["sweep_ms"], "insert_ms_total": st["insert_ms"],
+        "result_buffers": args.serve_buffers, "result": "extract: tree edges; epsilon-cut: labels (pinned host)",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,6 +292,11 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--flatten", type=int, default=0, help="sweep flatten divisor (0: autotune)")
     ap.add_argument("--block", type=int, default=0, help="sweep block size (0: autotune)")
+    ap.add_argument("--serve-workload", default="blobs4m_d16")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving window (0: skip the serving leg)")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-buffers", type=int, default=96, help="pinned host result buffers")
+    ap.add_argument("--serve-inserts-first", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -320,6 +418,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges)
 
+    serving = None
+    if args.serve_seconds > 0:
+        g.close()
+        serving = run_serving(cs, ctx, args)
+        log(f"[rank {rank}] serving {serving}")
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": world, "steps": args.steps,
@@ -332,6 +436,8 @@ def main():
             "build_s": build_s, "build": st,
             "plain": plain, "speedup_vs_plain": (value / world) / plain["value"] if plain else None,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "p50_query_ms": serving["p50_query_ms"] if serving else None,
+            "p99_query_ms": serving["p99_query_ms"] if serving else None, "serving": serving,
             "clocks": clocks, "wall_s_timed": wall,
         }
         print(json.dumps(line))

@@ -262,11 +262,14 @@ cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint3
  * and served in arrival order.  Consecutive queries are batched as they arrive:
  * every batch is one 32-lane graph-captured sweep over the distinct mpts it holds
  * (a query that arrives while a batch is on the GPU joins the next one), its
- * results are copied into device result slots in stream order, and a completion
- * thread copies the slots into the callers' host buffers on a second stream while
- * the next sweep runs.  An insert is a barrier: queries before it see the graph
- * without its rows, queries after it see them (CoreSG::insert, then the bridges are
- * re-selected).  Admission is by free HBM: a result slot is allocated only while
+ * results are copied into device result slots in stream order (one slot per
+ * distinct extract mpts, shared by its queries, and one per epsilon-cut), and a
+ * completion thread copies the slots into the callers' host buffers on a second
+ * stream while the next sweep runs.  Inserts that are queued back to back are
+ * applied as one batch (CoreSG::insert of their rows in order, then the bridges are
+ * re-selected).  In arrival order an insert is a barrier: queries before it see the
+ * graph without its rows, queries after it see them; with inserts_first, queued
+ * inserts go ahead of queued queries.  Admission is by free HBM: a result slot is allocated only while
  * cudaMemGetInfo leaves `reserve_bytes` free, otherwise the batch is cut short and
  * waits for slots in flight; an insert whose growth does not fit fails with
  * CS_ERR_OOM.  The graph must not be used through other entry points while a server
@@ -279,7 +282,12 @@ enum { CS_REQ_EXTRACT = 0, CS_REQ_EPS_LABELS = 1, CS_REQ_INSERT = 2 };
 
 typedef struct {
     uint32_t max_batch;       /* distinct mpts per sweep, 1..32 (0: 32) */
-    uint32_t max_slots;       /* result slots in flight (0: 64) */
+    uint32_t max_slots;       /* result slots allocated at most (0: 64) */
+    uint32_t inserts_first;   /* 0: arrival order, an insert is a barrier between the
+                                 queries before and after it; 1: every queued insert
+                                 is applied before the queued queries (a query sees
+                                 at least the inserts submitted before it) */
+    uint32_t reserved0;
     uint64_t reserve_bytes;   /* HBM left free by admission (0: 2 GiB) */
     cs_insert_params insert;  /* parameters of every insert (cs_insert_defaults if
                                  sample == 0) */
@@ -317,6 +325,7 @@ typedef struct {
     uint64_t batches;          /* sweeps run */
     uint64_t queries;          /* extract + epsilon-cut requests served */
     uint64_t inserts, inserted_rows;
+    uint64_t insert_batches;   /* knn inserts run (back-to-back inserts share one) */
     uint64_t slots, slot_bytes;  /* result slots allocated, bytes each */
     uint32_t max_batch_seen;   /* most requests served by one sweep */
     double sweep_ms;           /* device time of all sweeps */

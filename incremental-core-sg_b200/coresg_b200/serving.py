@@ -18,8 +18,8 @@ CS_REQ_EXTRACT, CS_REQ_EPS_LABELS, CS_REQ_INSERT = 0, 1, 2
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("max_batch", C.c_uint32), ("max_slots", C.c_uint32), ("reserve_bytes", C.c_uint64),
-                ("insert", InsertParams)]
+    _fields_ = [("max_batch", C.c_uint32), ("max_slots", C.c_uint32), ("inserts_first", C.c_uint32),
+                ("reserved0", C.c_uint32), ("reserve_bytes", C.c_uint64), ("insert", InsertParams)]
 
 
 class Request(C.Structure):
@@ -37,8 +37,9 @@ class Result(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("batches", C.c_uint64), ("queries", C.c_uint64), ("inserts", C.c_uint64),
-                ("inserted_rows", C.c_uint64), ("slots", C.c_uint64), ("slot_bytes", C.c_uint64),
-                ("max_batch_seen", C.c_uint32), ("sweep_ms", C.c_double), ("insert_ms", C.c_double)]
+                ("inserted_rows", C.c_uint64), ("insert_batches", C.c_uint64), ("slots", C.c_uint64),
+                ("slot_bytes", C.c_uint64), ("max_batch_seen", C.c_uint32), ("sweep_ms", C.c_double),
+                ("insert_ms", C.c_double)]
 
 
 class Pinned:
@@ -70,10 +71,12 @@ class Server:
     """cs_server over a resident CoreSG: submit extract / epsilon-cut / insert
     requests from any thread, wait on their tickets."""
 
-    def __init__(self, graph: CoreSG, max_batch=32, max_slots=64, reserve_bytes=0, **insert_params):
+    def __init__(self, graph: CoreSG, max_batch=32, max_slots=64, reserve_bytes=0, inserts_first=False,
+                 **insert_params):
         self.graph = graph
         cfg = ServerConfig()
         cfg.max_batch, cfg.max_slots, cfg.reserve_bytes = max_batch, max_slots, reserve_bytes
+        cfg.inserts_first = int(bool(inserts_first))
         lib().cs_insert_defaults(C.byref(cfg.insert))
         for key, val in insert_params.items():
             setattr(cfg.insert, key, val)

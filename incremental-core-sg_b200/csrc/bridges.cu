@@ -265,10 +265,35 @@ __global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* _
     if (threadIdx.x == 0) *out_count = s_cnt;
 }
 
+/// Views of the graph's cached selection scratch (grow-only buffers).
 struct Scratch {
-    DevBuf parent, lab, bc, ncomp, rdeg, score, ks, kt, hist, chosen, qtaken, sel, selcnt, best_s, best_t,
-        sub_pts, sub_core, mat, pbest, pfrom, pintree, pout, pcnt;
+    DevBuf &parent, &lab, &bc, &ncomp, &rdeg, &score, &ks, &kt, &hist, &chosen, &qtaken, &sel, &selcnt, &best_s,
+        &best_t, &sub_pts, &sub_core, &mat, &pbest, &pfrom, &pintree, &pout, &pcnt;
+    explicit Scratch(Graph& g)
+        : parent(g.bridge_scratch[0]), lab(g.bridge_scratch[1]), bc(g.bridge_scratch[2]), ncomp(g.bridge_scratch[3]),
+          rdeg(g.bridge_scratch[4]), score(g.bridge_scratch[5]), ks(g.bridge_scratch[6]), kt(g.bridge_scratch[7]),
+          hist(g.bridge_scratch[8]), chosen(g.bridge_scratch[9]), qtaken(g.bridge_scratch[10]),
+          sel(g.bridge_scratch[11]), selcnt(g.bridge_scratch[12]), best_s(g.bridge_scratch[13]),
+          best_t(g.bridge_scratch[14]), sub_pts(g.bridge_scratch[15]), sub_core(g.bridge_scratch[16]),
+          mat(g.bridge_scratch[17]), pbest(g.bridge_scratch[18]), pfrom(g.bridge_scratch[19]),
+          pintree(g.bridge_scratch[20]), pout(g.bridge_scratch[21]), pcnt(g.bridge_scratch[22]) {}
 };
+
+/// out[i] = (key_a[idx[i]], key_b[idx[i]]): the sort keys of the selected ids.
+__global__ void k_gather_keys(const uint32_t* __restrict__ idx, uint32_t m, const unsigned long long* __restrict__ a,
+                              const unsigned long long* __restrict__ b, unsigned long long* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    out[2 * i] = a[idx[i]];
+    out[2 * i + 1] = b[idx[i]];
+}
+
+/// out[i] = src[idx[i]].
+__global__ void k_gather_u32(const uint32_t* __restrict__ idx, uint32_t m, const uint32_t* __restrict__ src,
+                             uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = src[idx[i]];
+}
 
 /// Smallest threshold T over key[] (restricted by the filter) with
 /// count(key <= T) >= rank (1-based), by 8-bit radix passes from the top.
@@ -365,7 +390,7 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     const uint32_t n = static_cast<uint32_t>(g.n);
     const uint32_t k = g.k;
     CSB_REQUIRE(n > 0, "cs_select_bridges: empty graph");
-    Scratch s;
+    Scratch s(g);
     int* status = c.status.as<int>();
     CSB_CUDA(cudaMemsetAsync(status, 0, 4, c.stream));
     const uint64_t nk = static_cast<uint64_t>(n) * k;
@@ -435,7 +460,7 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
             uint64_t below = 0;
             // histogram-free count: reuse radix select on ks with rank = budget gives T;
             // the ties needed = budget - count(ks < T); count it with one more pass
-            DevBuf tmpc;
+            DevBuf& tmpc = s.pcnt;
             tmpc.ensure(64);
             CSB_CUDA(cudaMemsetAsync(tmpc.p, 0, 64, c.stream));
             k_collect<<<blocks_for(n), kThreads, 0, c.stream>>>(ks, kt, n, T, 0, 0, s.chosen.as<uint8_t>(),
@@ -479,33 +504,52 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     if (m > cap) fail(CS_ERR_STATE, "selection overflow");
     // order the (few hundred) selected ids by (score, rdeg, id) on the host
     std::vector<uint32_t> sel(m);
-    std::vector<unsigned long long> hks(n), hkt;
     copy_d2h(c, sel.data(), s.sel.p, m * 4ull);
-    {
-        std::vector<unsigned long long> sk(m), tk(m);
-        // gather the keys of the selected ids
-        std::vector<unsigned long long> all_ks(n), all_kt(n);
-        copy_d2h(c, all_ks.data(), s.ks.p, n * 8ull);
-        copy_d2h(c, all_kt.data(), s.kt.p, n * 8ull);
-        std::sort(sel.begin(), sel.end(), [&](uint32_t a, uint32_t b) {
-            if (all_ks[a] != all_ks[b]) return all_ks[a] < all_ks[b];
-            return all_kt[a] < all_kt[b];
+    if (m) {
+        DevBuf& tmp = c.scratch[6];
+        tmp.ensure(m * 16ull + 16);
+        k_gather_keys<<<blocks_for(m), kThreads, 0, c.stream>>>(s.sel.as<uint32_t>(), m, ks, kt,
+                                                                tmp.as<unsigned long long>());
+        count_launch(c);
+        std::vector<unsigned long long> keys(2ull * m);
+        copy_d2h(c, keys.data(), tmp.p, m * 16ull);
+        std::vector<uint32_t> order(m);
+        for (uint32_t i = 0; i < m; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            if (keys[2 * a] != keys[2 * b]) return keys[2 * a] < keys[2 * b];
+            return keys[2 * a + 1] < keys[2 * b + 1];
         });
-        hks.swap(all_ks);
-        hkt.swap(all_kt);
+        std::vector<uint32_t> sorted(m);
+        for (uint32_t i = 0; i < m; ++i) sorted[i] = sel[order[i]];
+        sel.swap(sorted);
     }
     g.selected = sel;
     copy_h2d(c, s.sel.p, sel.data(), m * 4ull);
     // ---- bridge MST over the selected set
     std::vector<cs_edge> missing;
     mst_over_subset(g, s, s.sel.as<uint32_t>(), m, &missing);
-    // ---- repair_connectivity
+    // ---- repair_connectivity (only a k-NN graph of several components needs it)
     uint64_t added = 0;
-    {
-        std::vector<uint32_t> lab(n);
-        copy_d2h(c, lab.data(), s.lab.p, n * 4ull);
+    if (ncomp > 1) {
+        // the component of every bridge endpoint, gathered on the device
+        std::vector<uint32_t> ends(2 * missing.size()), end_lab(2 * missing.size());
+        for (size_t i = 0; i < missing.size(); ++i) {
+            ends[2 * i] = missing[i].u;
+            ends[2 * i + 1] = missing[i].v;
+        }
+        if (!ends.empty()) {
+            DevBuf& tmp = c.scratch[6];
+            tmp.ensure(ends.size() * 8ull + 16);
+            uint32_t* d_idx = tmp.as<uint32_t>();
+            uint32_t* d_out = d_idx + ends.size();
+            copy_h2d(c, d_idx, ends.data(), ends.size() * 4);
+            k_gather_u32<<<blocks_for(ends.size()), kThreads, 0, c.stream>>>(
+                d_idx, static_cast<uint32_t>(ends.size()), s.lab.as<uint32_t>(), d_out);
+            count_launch(c);
+            copy_d2h(c, end_lab.data(), d_out, ends.size() * 4);
+        }
         HostUF uf(ncomp);
-        for (const cs_edge& e : missing) uf.unite(lab[e.u], lab[e.v]);
+        for (size_t i = 0; i < missing.size(); ++i) uf.unite(end_lab[2 * i], end_lab[2 * i + 1]);
         // merged dense labels, numbered by first component (UnionFind::labels)
         std::vector<uint32_t> merged(ncomp), remap(ncomp, kInvalid);
         uint32_t nc2 = 0;
@@ -515,6 +559,8 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
             merged[cc] = remap[r];
         }
         if (nc2 > 1) {
+            std::vector<uint32_t> lab(n);
+            copy_d2h(c, lab.data(), s.lab.p, n * 4ull);
             std::vector<double> score(n);
             copy_d2h(c, score.data(), s.score.p, n * 8ull);
             uint64_t per = 4;

@@ -43,6 +43,9 @@ void DevBuf::release() {
 
 void DevBuf::ensure(size_t nbytes) {
     if (nbytes <= bytes && p) return;
+    // a buffer that grows again (resident arrays after inserts) takes a quarter of
+    // headroom, so a run of small growths does not reallocate every time
+    if (p) nbytes = std::max(nbytes, bytes + bytes / 4);
     release();
     if (nbytes == 0) nbytes = 16;
     void* q = nullptr;

@@ -117,6 +117,12 @@ struct Graph {
         DevBuf eu, ev, ew, core, parent, best, touched, wl, bitmap, bins, ctr, tiles, lab, out, counts;
     } plain;
 
+    // Scratch kept across calls (grow-only): NN-Descent (knn.cu), the insert path's
+    // search and active sets (knn.cu), the bridge selection (bridges.cu).
+    DevBuf knn_scratch[13];
+    DevBuf insert_scratch[12];
+    DevBuf bridge_scratch[23];
+
     // Hubness selection of the last cs_select_bridges.
     std::vector<uint32_t> selected;
 

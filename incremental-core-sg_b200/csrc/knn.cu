@@ -698,8 +698,14 @@ __global__ void k_rev_keys(const uint32_t* __restrict__ ids, const uint32_t* __r
     keys[x] = key;
 }
 
+/// Views of the graph's cached descent scratch (grow-only buffers).
 struct KnnScratch {
-    DevBuf thr, cand, cand_buf, cand_cnt, new_s, old_s, ns, nold, rnew, rold, rnew_cnt, rold_cnt, counters;
+    DevBuf &thr, &cand, &cand_buf, &cand_cnt, &new_s, &old_s, &ns, &nold, &rnew, &rold, &rnew_cnt, &rold_cnt, &counters;
+    explicit KnnScratch(Graph& g)
+        : thr(g.knn_scratch[0]), cand(g.knn_scratch[1]), cand_buf(g.knn_scratch[2]), cand_cnt(g.knn_scratch[3]),
+          new_s(g.knn_scratch[4]), old_s(g.knn_scratch[5]), ns(g.knn_scratch[6]), nold(g.knn_scratch[7]),
+          rnew(g.knn_scratch[8]), rold(g.knn_scratch[9]), rnew_cnt(g.knn_scratch[10]), rold_cnt(g.knn_scratch[11]),
+          counters(g.knn_scratch[12]) {}
 };
 
 CandStore store_of(KnnScratch& s) {
@@ -742,7 +748,7 @@ struct Descent {
     unsigned long long* d_updates = nullptr;
     unsigned long long* d_evals = nullptr;
 
-    Descent(Graph& graph, uint32_t sample) : g(graph), c(*graph.ctx) {
+    Descent(Graph& graph, uint32_t sample) : g(graph), c(*graph.ctx), s(graph) {
         n = static_cast<uint32_t>(g.n);
         k = g.k;
         smp = std::min<uint32_t>(std::max<uint32_t>(sample, 1), kMaxSample);
@@ -900,14 +906,19 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     // seeding search over the base graph (ef = 2k results, at most the 64-entry
     // pool; the selected anti-hubs as extra entry points), then the seeds both ways
     const uint32_t width = std::min<uint32_t>(2 * k, 64);
-    DevBuf seeds, hints;
+    DevBuf& seeds = g.insert_scratch[0];
+    DevBuf& hints = g.insert_scratch[1];
     seeds.ensure(static_cast<uint64_t>(nn) * width * 8);
     const uint32_t n_hint = static_cast<uint32_t>(g.selected.size());
     if (n_hint) {
         hints.ensure(n_hint * 4ull);
         copy_h2d(c, hints.p, g.selected.data(), n_hint * 4ull);
     }
-    DevBuf rev_keys, rev_alt, rev_deg, rev_off, sort_tmp;
+    DevBuf& rev_keys = g.insert_scratch[2];
+    DevBuf& rev_alt = g.insert_scratch[3];
+    DevBuf& rev_deg = g.insert_scratch[4];
+    DevBuf& rev_off = g.insert_scratch[5];
+    DevBuf& sort_tmp = g.insert_scratch[6];
     if (p.reverse_cap) {
         const uint64_t nk = static_cast<uint64_t>(first_new) * k;
         CSB_REQUIRE(nk < 0x7FFFFFFFull, "cs_insert: base graph too large for the reverse index");
@@ -930,7 +941,10 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
         sort_tmp.ensure(tmp_bytes + 16);
         CSB_CUDA(cub::DeviceRadixSort::SortKeys(sort_tmp.p, tmp_bytes, db, static_cast<int>(nk), 0, end_bit, c.stream));
         count_launch(c, static_cast<uint64_t>((end_bit + 7) / 8) + 1);  // histogram + one per digit
-        if (db.Current() != rev_keys.as<unsigned long long>()) std::swap(rev_keys.p, rev_alt.p);
+        if (db.Current() != rev_keys.as<unsigned long long>()) {
+            std::swap(rev_keys.p, rev_alt.p);
+            std::swap(rev_keys.bytes, rev_alt.bytes);
+        }
         scan_u32(c, rev_deg.as<uint32_t>(), rev_off.as<uint32_t>(), first_new);
         check_launch(c, "insert reverse index");
     }
@@ -946,7 +960,11 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     launch_merge(c, g, d.s, nullptr);
     check_launch(c, "insert seeding");
     CSB_CUDA(cudaEventRecord(e1, c.stream));
-    DevBuf mark, firstpos, active, flag, off;
+    DevBuf& mark = g.insert_scratch[7];
+    DevBuf& firstpos = g.insert_scratch[8];
+    DevBuf& active = g.insert_scratch[9];
+    DevBuf& flag = g.insert_scratch[10];
+    DevBuf& off = g.insert_scratch[11];
     mark.ensure(n + 16ull);
     firstpos.ensure(n * 4ull);
     active.ensure(static_cast<uint64_t>(n) * 4 + 4);

@@ -4,10 +4,14 @@
 //   scheduler   takes requests in arrival order.  A run of consecutive queries
 //               (extract / epsilon-cut) becomes one batch: one 32-lane sweep over
 //               its distinct mpts values (the plan is captured once and replayed;
-//               unused lanes repeat a value), after which every query's tree, labels
-//               and exact-sum bins are copied into a result slot in HBM, in stream
-//               order, and epsilon-cuts are labelled on the device.  An insert is a
-//               barrier between batches (CoreSG::insert, src/coresg.cpp:325-389).
+//               unused lanes repeat a value), after which each distinct extract
+//               mpts has its tree, labels and exact-sum bins copied into one result
+//               slot in HBM that its queries share, in stream order, and every
+//               epsilon-cut is labelled on the device into a slot of its own.
+//               Inserts queued back to back are applied as one batch; in arrival
+//               order they are a barrier between batches (CoreSG::insert,
+//               src/coresg.cpp:325-389), with inserts_first they go ahead of the
+//               queued queries.
 //   completion  waits for a batch's event and copies its slots into the callers'
 //               host buffers on its own stream, while the scheduler already runs
 //               the next sweep on the context stream.
@@ -80,6 +84,7 @@ struct Req {
 struct Batch {
     uint64_t id = 0;
     std::vector<Req*> reqs;
+    std::vector<Slot*> slots;  // owned until the batch's copies finish
     cudaEvent_t ready = nullptr;
     uint64_t n = 0;
 };
@@ -164,17 +169,21 @@ struct Server {
         st.slots = all_slots.size();
     }
 
-    void run_insert(Req* q);
+    void run_inserts(std::vector<Req*>& batch);
     void run_batch(std::vector<Req*>& take);
     void sched_loop();
     void comp_loop();
 };
 
-void Server::run_insert(Req* q) {
+void Server::run_inserts(std::vector<Req*>& batch) {
     const double t0 = now_ms();
+    uint64_t rows_total = 0;
     {
         std::lock_guard<std::mutex> lk(mu);
-        q->res.queue_ms = t0 - q->t_submit;
+        for (Req* q : batch) {
+            q->res.queue_ms = t0 - q->t_submit;
+            rows_total += q->r.count;
+        }
     }
     cs_status status = CS_OK;
     std::string msg;
@@ -183,9 +192,9 @@ void Server::run_insert(Req* q) {
         try {
             c->bind();
             // admission: the growth of the resident arrays and the descent scratch
-            const uint64_t n1 = g->n + q->r.count;
+            const uint64_t n1 = g->n + rows_total;
             const uint64_t need = n1 * (static_cast<uint64_t>(g->stride) * 4 + g->k * 9ull + 2600) +
-                                  q->r.count * 64ull * 8;
+                                  rows_total * 64ull * 8;
             size_t free_b = 0, total_b = 0;
             CSB_CUDA(cudaMemGetInfo(&free_b, &total_b));
             if (free_b < need + cfg.reserve_bytes) {
@@ -198,9 +207,28 @@ void Server::run_insert(Req* q) {
                 if (free_b < need + cfg.reserve_bytes)
                     fail(CS_ERR_OOM, "insert not admitted: free HBM below the batch's growth plus the reserve");
             }
-            InsertStats ist;
-            knn_insert(*g, q->rows.data(), q->r.count, q->r.row_stride, cfg.insert, &ist);
-            if (cfg.insert.reselect_bridges) select_bridges(*g, nullptr, nullptr, nullptr, nullptr);
+            // back-to-back inserts are one batch: their rows in submission order
+            const uint32_t dim = g->dim;
+            const float* rows = nullptr;
+            uint32_t stride = dim;
+            std::vector<float> joined;
+            if (batch.size() == 1) {
+                rows = batch[0]->rows.data();
+                stride = batch[0]->r.row_stride;
+            } else {
+                joined.resize(rows_total * dim);
+                uint64_t at = 0;
+                for (Req* q : batch) {
+                    for (uint64_t i = 0; i < q->r.count; ++i, ++at)
+                        std::memcpy(joined.data() + at * dim, q->rows.data() + i * q->r.row_stride, dim * 4);
+                }
+                rows = joined.data();
+            }
+            if (rows_total) {
+                InsertStats ist;
+                knn_insert(*g, rows, rows_total, stride, cfg.insert, &ist);
+                if (cfg.insert.reselect_bridges) select_bridges(*g, nullptr, nullptr, nullptr, nullptr);
+            }
         } catch (const Error& e) {
             status = e.status;
             msg = e.what();
@@ -212,27 +240,45 @@ void Server::run_insert(Req* q) {
     std::lock_guard<std::mutex> lk(mu);
     st.insert_ms += now_ms() - t0;
     if (status == CS_OK) {
-        ++st.inserts;
-        st.inserted_rows += q->r.count;
-    } else {
-        set_error(q, status, msg);
+        st.inserts += batch.size();
+        st.inserted_rows += rows_total;
+        ++st.insert_batches;
     }
-    q->res.n = g->n;
-    finish(q);
+    for (Req* q : batch) {
+        if (status != CS_OK) set_error(q, status, msg);
+        q->res.n = g->n;
+        finish(q);
+    }
     cv.notify_all();
 }
 
 void Server::run_batch(std::vector<Req*>& take) {
     const uint64_t n = g->n;
-    // result slots, admitted by free memory; a batch that cannot get all of them is
-    // cut short and the rest goes back to the head of the queue
+    // result slots, admitted by free memory: one per distinct extract mpts (its
+    // queries share the tree) and one per epsilon-cut.  A batch that cannot get a
+    // slot it needs is cut short there and the rest goes back to the queue head.
+    std::vector<Slot*> slots;
+    std::vector<std::pair<uint32_t, Slot*>> trees;  // extract mpts -> shared slot
     size_t got = 0;
     {
         std::unique_lock<std::mutex> lk(mu);
         while (got < take.size()) {
-            Slot* s = try_slot(n);
-            if (s) {
-                take[got++]->slot = s;
+            Req* q = take[got];
+            const uint32_t m = std::max<uint32_t>(q->r.mpts, 1);
+            if (q->r.kind == CS_REQ_EXTRACT) {
+                auto it = std::find_if(trees.begin(), trees.end(), [&](const auto& t) { return t.first == m; });
+                if (it != trees.end()) {
+                    q->slot = it->second;
+                    ++got;
+                    continue;
+                }
+            }
+            Slot* sl = try_slot(n);
+            if (sl) {
+                slots.push_back(sl);
+                if (q->r.kind == CS_REQ_EXTRACT) trees.emplace_back(m, sl);
+                q->slot = sl;
+                ++got;
                 continue;
             }
             if (got > 0) break;  // serve what fits now
@@ -265,6 +311,7 @@ void Server::run_batch(std::vector<Req*>& take) {
     Batch* b = new Batch;
     b->n = n;
     b->reqs = take;
+    b->slots = slots;
     cs_status status = CS_OK;
     std::string msg;
     float ms = 0.0f;
@@ -273,19 +320,31 @@ void Server::run_batch(std::vector<Req*>& take) {
         try {
             c->bind();
             sweep_run(*g, lanes.data(), kSweepLanes, true, &ms);
-            for (Req* q : take) {
+            // every slot is filled once: a shared tree slot by its first query, with
+            // the edges / labels any of its queries asked for
+            for (size_t i = 0; i < take.size(); ++i) {
+                Req* q = take[i];
+                Slot* sl = q->slot;
+                bool first = true;
+                for (size_t j = 0; j < i; ++j) first = first && take[j]->slot != sl;
+                if (!first) continue;
                 const SweepOut o = sweep_outputs(*g, q->lane);
-                Slot* s = q->slot;
-                unsigned long long* meta = s->meta.as<unsigned long long>();
+                unsigned long long* meta = sl->meta.as<unsigned long long>();
                 CSB_CUDA(cudaMemsetAsync(meta, 0, kMetaWords * 8, c->stream));
                 CSB_CUDA(cudaMemcpyAsync(meta, o.count, 8, cudaMemcpyDeviceToDevice, c->stream));
                 CSB_CUDA(cudaMemcpyAsync(meta + 2, o.bins, 256 * 8, cudaMemcpyDeviceToDevice, c->stream));
                 if (q->r.kind == CS_REQ_EXTRACT) {
-                    if (q->r.out_edges && o.cap)
-                        CSB_CUDA(cudaMemcpyAsync(s->edges.p, o.edges, o.cap * sizeof(cs_edge), cudaMemcpyDeviceToDevice,
+                    bool edges = false, labels = false;
+                    for (size_t j = i; j < take.size(); ++j) {
+                        if (take[j]->slot != sl) continue;
+                        edges = edges || take[j]->r.out_edges;
+                        labels = labels || take[j]->r.out_labels;
+                    }
+                    if (edges && o.cap)
+                        CSB_CUDA(cudaMemcpyAsync(sl->edges.p, o.edges, o.cap * sizeof(cs_edge), cudaMemcpyDeviceToDevice,
                                                  c->stream));
-                    if (q->r.out_labels && n)
-                        CSB_CUDA(cudaMemcpyAsync(s->labels.p, o.labels, n * 4, cudaMemcpyDeviceToDevice, c->stream));
+                    if (labels && n)
+                        CSB_CUDA(cudaMemcpyAsync(sl->labels.p, o.labels, n * 4, cudaMemcpyDeviceToDevice, c->stream));
                 } else if (n) {  // epsilon-cut of this tree, labelled into the slot
                     cut_parent.ensure(n * 4);
                     cut_tiles.ensure((blocks_for(n) + 2) * 4ull + 64);
@@ -296,7 +355,7 @@ void Server::run_batch(std::vector<Req*>& take) {
                             o.edges, o.count, o.cap, q->r.eps, cut_parent.as<uint32_t>(),
                             reinterpret_cast<int*>(meta + 258));
                     count_launch(*c, 2);
-                    launch_labels(*c, cut_parent.as<uint32_t>(), static_cast<uint32_t>(n), 1, s->labels.as<uint32_t>(),
+                    launch_labels(*c, cut_parent.as<uint32_t>(), static_cast<uint32_t>(n), 1, sl->labels.as<uint32_t>(),
                                   cut_tiles.as<uint32_t>(), meta + 1);
                 }
             }
@@ -316,10 +375,10 @@ void Server::run_batch(std::vector<Req*>& take) {
         for (Req* q : take) {
             set_error(q, status, msg);
             q->res.n = n;
-            free_slots.push_back(q->slot);
             q->slot = nullptr;
             finish(q);
         }
+        for (Slot* sl : slots) free_slots.push_back(sl);
         if (b->ready) cudaEventDestroy(b->ready);
         delete b;
         cv.notify_all();
@@ -343,23 +402,45 @@ void Server::sched_loop() {
             if (stop_sched) return;
             continue;
         }
-        Req* front = queue.front();
-        if (front->r.kind == CS_REQ_INSERT) {
-            // a barrier: the batches before it finish their sweeps first (they
-            // already have; sweeps are synchronous), then the graph changes
-            queue.pop_front();
+        // inserts: the run at the head of the queue (arrival order: a barrier after
+        // the sweeps already dispatched), or every queued one (inserts_first)
+        std::vector<Req*> ins;
+        if (cfg.inserts_first) {
+            for (auto it = queue.begin(); it != queue.end();) {
+                if ((*it)->r.kind == CS_REQ_INSERT) {
+                    ins.push_back(*it);
+                    it = queue.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        } else {
+            while (!queue.empty() && queue.front()->r.kind == CS_REQ_INSERT) {
+                ins.push_back(queue.front());
+                queue.pop_front();
+            }
+        }
+        if (!ins.empty()) {
             lk.unlock();
-            run_insert(front);
+            run_inserts(ins);
             continue;
         }
+        // the run of queries at the head: at most max_batch distinct mpts and
+        // max_slots slots (a distinct extract mpts or an epsilon-cut takes one)
         std::vector<Req*> take;
-        std::vector<uint32_t> distinct;
-        while (!queue.empty() && queue.front()->r.kind != CS_REQ_INSERT && take.size() < cfg.max_slots) {
+        std::vector<uint32_t> distinct, trees;
+        uint32_t need = 0;
+        while (!queue.empty() && queue.front()->r.kind != CS_REQ_INSERT) {
             Req* q = queue.front();
             const uint32_t m = std::max<uint32_t>(q->r.mpts, 1);
-            if (std::find(distinct.begin(), distinct.end(), m) == distinct.end()) {
-                if (distinct.size() >= cfg.max_batch) break;
-                distinct.push_back(m);
+            const bool new_m = std::find(distinct.begin(), distinct.end(), m) == distinct.end();
+            const bool new_slot =
+                q->r.kind != CS_REQ_EXTRACT || std::find(trees.begin(), trees.end(), m) == trees.end();
+            if ((new_m && distinct.size() >= cfg.max_batch) || (new_slot && need >= cfg.max_slots)) break;
+            if (new_m) distinct.push_back(m);
+            if (new_slot) {
+                ++need;
+                if (q->r.kind == CS_REQ_EXTRACT) trees.push_back(m);
             }
             take.push_back(q);
             queue.pop_front();
@@ -433,10 +514,10 @@ void Server::comp_loop() {
         for (Req* q : b->reqs) {
             if (err != cudaSuccess && q->res.status == CS_OK)
                 set_error(q, CS_ERR_CUDA, std::string("result copy: ") + cudaGetErrorString(err));
-            free_slots.push_back(q->slot);
             q->slot = nullptr;
             finish(q);
         }
+        for (Slot* sl : b->slots) free_slots.push_back(sl);
         inflight.pop_front();
         cudaEventDestroy(b->ready);
         delete b;

@@ -608,9 +608,23 @@ bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
 uint64_t kernels_pre() { return 1; }
 uint64_t kernels_post(const SweepPlan& p) { return (p.labels ? 4 : 0) + 4; }
 
-SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div, bool labels) {
+/// A plan for the graph's current shape.  `reuse` (a plan that no longer matches)
+/// gives its buffers, which only grow, so a graph that grows by inserts recaptures
+/// its graphs without reallocating every buffer; it is consumed either way.
+SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div, bool labels, SweepPlan* reuse) {
     Ctx& c = *g.ctx;
-    SweepPlan* p = new SweepPlan();
+    SweepPlan* p = reuse ? reuse : new SweepPlan();
+    if (reuse) {
+        if (p->exec_pre) cudaGraphExecDestroy(p->exec_pre);
+        if (p->exec_main) cudaGraphExecDestroy(p->exec_main);
+        if (p->exec_post) cudaGraphExecDestroy(p->exec_post);
+        if (p->ev_k0) cudaEventDestroy(p->ev_k0);
+        if (p->ev_k1) cudaEventDestroy(p->ev_k1);
+        p->exec_pre = p->exec_main = p->exec_post = nullptr;
+        p->ev_k0 = p->ev_k1 = nullptr;
+        delete p->next;
+        p->next = nullptr;
+    }
     try {
         p->n = static_cast<uint32_t>(g.n);
         p->E = static_cast<uint32_t>(g.e_total);
@@ -733,11 +747,13 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
     for (uint32_t off = 0; off < K; off += kLanes) {
         const uint32_t Kp = std::min<uint32_t>(kLanes, K - off);
         if (!plan_matches(*slot, g, Kp, B, F, want_labels)) {
-            SweepPlan* nxt = *slot ? (*slot)->next : nullptr;
-            if (*slot) (*slot)->next = nullptr;
-            sweep_free(*slot);
-            *slot = make_plan(g, Kp, B, F, want_labels);
-            (*slot)->next = nxt;
+            SweepPlan* old = *slot;
+            SweepPlan* nxt = old ? old->next : nullptr;
+            if (old) old->next = nullptr;
+            *slot = nxt;  // keeps the chain owned if the plan cannot be made
+            SweepPlan* np = make_plan(g, Kp, B, F, want_labels, old);
+            np->next = nxt;
+            *slot = np;
         }
         (*slot)->host_mpts.assign(mpts + off, mpts + off + Kp);
         for (auto& m : (*slot)->host_mpts) {

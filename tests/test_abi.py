@@ -47,8 +47,8 @@ def test_server_structs_match_the_header_layout():
 
     assert C.sizeof(Request) == 72 and Request.eps.offset == 8 and Request.out_labels_cap.offset == 64
     assert C.sizeof(Result) == 216 and Result.weight.offset == 24 and Result.error.offset == 56
-    assert C.sizeof(ServerConfig) == 96 and ServerConfig.insert.offset == 16
-    assert C.sizeof(Stats) == 96 and Stats.sweep_ms.offset == 80
+    assert C.sizeof(ServerConfig) == 104 and ServerConfig.insert.offset == 24
+    assert C.sizeof(Stats) == 104 and Stats.sweep_ms.offset == 88
 
 
 def test_request_stream_is_seeded_and_shaped():

@@ -158,3 +158,44 @@ def test_request_errors(gpu_ctx):
     r = srv.wait(srv.extract(8))
     assert r["status"] == 0 and r["weight"] == g.mst(8).weight
     srv.close()
+
+
+def test_back_to_back_inserts_coalesce_and_inserts_first(gpu_ctx):
+    """Inserts queued back to back run as one insert; with inserts_first a query
+    submitted after an insert sees it, and every result equals the alone result on
+    the graph state it reports."""
+    z = load_golden("coresg_n6000_d16_k32")
+    n0 = len(z["counts"])
+    rng = np.random.default_rng(11)
+    rows = [rng.normal(4.0, 1.0, size=(s, int(z["dim"]))).astype(np.float32) for s in (120, 300, 80)]
+    n1 = n0 + sum(len(r) for r in rows)
+    # arrival order: the first (slow, plan-capturing) sweep lets the inserts queue up
+    g = resident(gpu_ctx, z)
+    srv = cs.Server(g)
+    t0 = srv.extract(4)
+    ti = [srv.insert(r) for r in rows]
+    t1 = srv.extract(4)
+    r0, ri, r1 = srv.wait(t0), [srv.wait(t) for t in ti], srv.wait(t1)
+    st = srv.stats()
+    srv.close()
+    assert r0["n"] == n0 and all(r["status"] == 0 and r["n"] == n1 for r in ri) and r1["n"] == n1
+    assert st["inserts"] == 3 and st["insert_batches"] == 1 and st["inserted_rows"] == n1 - n0
+    assert r1["weight"] == g.mst(4).weight
+    # inserts first: queued inserts overtake queued queries, never the other way round
+    g2 = resident(gpu_ctx, z)
+    pre = g2.mst(8)
+    srv = cs.Server(g2, inserts_first=True)
+    e0, l0 = bufs(n1)
+    t0 = srv.extract(8, e0, l0)
+    ti = [srv.insert(r) for r in rows]
+    e1, l1 = bufs(n1)
+    t1 = srv.extract(8, e1, l1)
+    r0, ri, r1 = srv.wait(t0), [srv.wait(t) for t in ti], srv.wait(t1)
+    srv.close()
+    post = g2.mst(8)
+    assert r1["n"] == n1  # submitted after every insert
+    for r, e, lab in ((r0, e0, l0), (r1, e1, l1)):
+        want = pre if r["n"] == n0 else post
+        assert r["n"] in (n0, n1)
+        assert e[: r["nedges"]].tobytes() == want.edges.tobytes()
+        assert np.array_equal(lab[: r["n"]], want.component) and r["weight"] == want.weight
