@@ -73,20 +73,14 @@ struct SweepArgs {
     uint32_t* tree;            // [E] bit j: edge in MST j
     uint32_t* live;            // [E] bit j: edge live in MST j
     uint32_t* wl;              // [2][E]
-    uint32_t* tlist;           // [n]
-    uint32_t* tflag;           // [n]
-    uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] touched counts; [4] rounds
+    uint32_t* rlist;           // [2][n] roots that took an offer in the previous round
+    const float* core;         // [n][32] core distance of v at mpts[j]
+    uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] root-list counts; [4] rounds;
+                               // [5],[6] "some edge offered" flags
     unsigned* bar;
     int* status;
     uint64_t limit_ns;
 };
-
-__device__ __forceinline__ float core_lane(const SweepArgs& a, uint32_t x, uint32_t m) {
-    const uint32_t c = __ldg(a.counts + x);
-    if (c == 0) return __int_as_float(0x7f800000);
-    const uint32_t pos = (m < c ? m : c) - 1;  // m >= 1
-    return __ldg(a.dists + static_cast<uint64_t>(x) * a.k + pos);
-}
 
 /// find with path halving on forest j of the node-major parent array.
 __device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_t j) {
@@ -159,46 +153,46 @@ struct WarpList {
     }
 };
 
-/// Record roots offered to for the first time this round (warp-collective).
-__device__ __forceinline__ void touch(const SweepArgs& a, bool t, uint32_t root, WarpList& tl) {
-    const unsigned tm = __ballot_sync(0xFFFFFFFFu, t);
-    if (!tm) return;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned grp = __match_any_sync(0xFFFFFFFFu, t ? root : kInvalid) & tm;
-    bool first = false;
-    if (t && static_cast<int>(lane) == __ffs(grp) - 1) first = atomicOr(a.tflag + root, grp) == 0u;
-    tl.push(first, root);
+constexpr int kUnroll = 4;  // edges in flight per warp in the node-segment rounds
+
+/// Root of x in forest j for round r (the identity in round 0; one load when the
+/// forests are flat).
+__device__ __forceinline__ uint32_t root_of(const SweepArgs& a, uint32_t x, unsigned lane, int r, bool flat) {
+    if (r == 0) return x;
+    return flat ? __ldcg(a.parent + static_cast<uint64_t>(x) * kLanes + lane) : find32(a.parent, x, lane);
 }
 
-/// Phase A for one edge whose live lanes are `lm` (warp-collective).
-__device__ __forceinline__ void edge_lanes(const SweepArgs& a, uint32_t i, uint32_t lm, int r, bool flat,
-                                           uint32_t mj, WarpList& tl, WarpList& wlo) {
+/// Offer `key` to best[root][lane].  The old value is not needed (phase B finds the
+/// offered roots through the root list), so the atomic is issued without a return.
+__device__ __forceinline__ void offer_min(const SweepArgs& a, uint32_t root, unsigned lane, unsigned long long key) {
+    atomicMin(a.best + static_cast<uint64_t>(root) * kLanes + lane, key);
+}
+
+/// Phase A for one edge (i, u, v, w) whose live lanes are `lm` (warp-collective).
+/// With `track`, the edge's new live lanes are stored (always when `fresh`: the
+/// word still holds a previous sweep's value) and a live edge is pushed to the next
+/// worklist.  Returns whether this lane offered.
+__device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, uint32_t lm,
+                                           int r, bool flat, bool act, WarpList& wlo, bool track, bool fresh) {
     const unsigned lane = threadIdx.x & 31u;
-    const uint32_t u = __ldg(a.eu + i), v = __ldg(a.ev + i);
-    const float w = __ldg(a.ew + i);
-    const bool act = (lm >> lane) & 1u;
-    bool live = false, tu = false, tv = false;
-    uint32_t ru = u, rv = v;
-    if (act && u < a.n && v < a.n) {
-        const float wp = max_ref(w, max_ref(core_lane(a, u, mj), core_lane(a, v, mj)));
-        if (r > 0) {
-            ru = flat ? __ldcg(a.parent + static_cast<uint64_t>(u) * kLanes + lane) : find32(a.parent, u, lane);
-            rv = flat ? __ldcg(a.parent + static_cast<uint64_t>(v) * kLanes + lane) : find32(a.parent, v, lane);
-        }
+    bool live = false;
+    if (act && ((lm >> lane) & 1u) && u < a.n && v < a.n) {
+        const float cu = __ldg(a.core + static_cast<uint64_t>(u) * kLanes + lane);
+        const float cv = __ldg(a.core + static_cast<uint64_t>(v) * kLanes + lane);
+        const uint32_t ru = root_of(a, u, lane, r, flat), rv = root_of(a, v, lane, r, flat);
         live = ru != rv;
         if (live) {
-            const unsigned long long key = pack_key(wp, i);
-            tu = atomicMin(a.best + static_cast<uint64_t>(ru) * kLanes + lane, key) == kNoKey;
-            tv = atomicMin(a.best + static_cast<uint64_t>(rv) * kLanes + lane, key) == kNoKey;
+            const unsigned long long key = pack_key(max_ref(w, max_ref(cu, cv)), i);
+            offer_min(a, ru, lane, key);
+            offer_min(a, rv, lane, key);
         }
     }
-    touch(a, tu, ru, tl);
-    touch(a, tv, rv, tl);
-    if (r >= 1) {
+    if (track) {
         const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
-        if (L && lane == 0) a.live[i] = L;
+        if (L && (fresh || L != lm) && lane == 0) a.live[i] = L;
         wlo.push(L != 0 && lane == 0, i);
     }
+    return live;
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
@@ -208,87 +202,142 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const bool act = lane < a.K;
-    const uint32_t mj = act ? __ldg(a.mpts + lane) : 1u;
     const uint32_t allmask = a.K >= 32 ? 0xFFFFFFFFu : ((1u << a.K) - 1u);
     bool flat = true;  // parents are the identity at the start
     int r = 0;
     for (; r < kMaxRounds; ++r) {
-        const int par = r & 1;
-        WarpList tl{s_stage[wib][0], a.tlist, a.ctr + 2 + par, 0};
-        WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>((r + 1) & 1) * a.E, a.ctr + ((r + 1) & 1), 0};
+        const int par = r & 1, nxt = (r + 1) & 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.ctr[2 + nxt] = 0;  // the root list phase B of this round writes
+            a.ctr[5 + nxt] = 0;  // next round's offer flag
+        }
+        WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>(nxt) * a.E, a.ctr + nxt, 0};
+        bool offered = false;
         // ---- phase A
         if (r <= 1) {
-            // k-NN edges, node by node: the emitter's roots and core distances are
-            // loaded once, its offers are reduced in registers over its segment
+            // k-NN edges, node by node over the emitted segments: 32 edges of a
+            // segment are loaded at once, kUnroll of them are in flight, and the
+            // emitter's offers are reduced in registers and issued once
             for (uint32_t p = gw; p < a.n; p += nw) {
                 const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
                 if (beg == end) continue;
-                const float cp = act ? core_lane(a, p, mj) : 0.0f;
-                uint32_t rp = p;
-                if (r > 0 && act) rp = flat ? __ldcg(a.parent + static_cast<uint64_t>(p) * kLanes + lane) : find32(a.parent, p, lane);
+                const float cp = act ? __ldg(a.core + static_cast<uint64_t>(p) * kLanes + lane) : 0.0f;
+                const uint32_t rp = act ? root_of(a, p, lane, r, flat) : p;
                 unsigned long long seg = kNoKey;
-                for (uint32_t i = beg; i < end; ++i) {
-                    const uint32_t eu = __ldg(a.eu + i), ev = __ldg(a.ev + i);
-                    const float w = __ldg(a.ew + i);
-                    const uint32_t q = eu == p ? ev : eu;
-                    bool live = false, tq = false;
-                    uint32_t rq = q;
-                    if (act) {
-                        const float wp = max_ref(w, max_ref(cp, core_lane(a, q, mj)));
-                        if (r > 0) rq = flat ? __ldcg(a.parent + static_cast<uint64_t>(q) * kLanes + lane) : find32(a.parent, q, lane);
-                        live = rp != rq;
-                        if (live) {
-                            const unsigned long long key = pack_key(wp, i);
-                            seg = key < seg ? key : seg;
-                            tq = atomicMin(a.best + static_cast<uint64_t>(rq) * kLanes + lane, key) == kNoKey;
+                for (uint32_t b = beg; b < end; b += 32) {
+                    const uint32_t m = min(32u, end - b);
+                    uint32_t my_q = 0;
+                    float my_w = 0.0f;
+                    if (lane < m) {
+                        const uint32_t x = __ldg(a.eu + b + lane), y = __ldg(a.ev + b + lane);
+                        my_q = x == p ? y : x;
+                        my_w = __ldg(a.ew + b + lane);
+                    }
+                    for (uint32_t t = 0; t < m; t += kUnroll) {
+                        uint32_t q[kUnroll], rq[kUnroll];
+                        float w[kUnroll], cq[kUnroll];
+                        bool ok[kUnroll], lv[kUnroll];
+#pragma unroll
+                        for (int x = 0; x < kUnroll; ++x) {
+                            q[x] = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
+                            w[x] = __shfl_sync(0xFFFFFFFFu, my_w, (t + x) & 31u);
+                            ok[x] = act && t + x < m && q[x] < a.n;
+                        }
+#pragma unroll
+                        for (int x = 0; x < kUnroll; ++x)
+                            cq[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(q[x]) * kLanes + lane) : 0.0f;
+#pragma unroll
+                        for (int x = 0; x < kUnroll; ++x) rq[x] = ok[x] ? root_of(a, q[x], lane, r, flat) : rp;
+#pragma unroll
+                        for (int x = 0; x < kUnroll; ++x) {
+                            lv[x] = ok[x] && rp != rq[x];
+                            if (lv[x]) {
+                                const unsigned long long key = pack_key(max_ref(w[x], max_ref(cp, cq[x])), b + t + x);
+                                seg = key < seg ? key : seg;
+                                offer_min(a, rq[x], lane, key);
+                            }
+                        }
+                        if (r == 1) {
+#pragma unroll
+                            for (int x = 0; x < kUnroll; ++x) {
+                                if (t + x < m) {
+                                    const unsigned L = __ballot_sync(0xFFFFFFFFu, lv[x]);
+                                    if (L && lane == 0) a.live[b + t + x] = L;
+                                    wlo.push(L != 0 && lane == 0, b + t + x);
+                                }
+                            }
                         }
                     }
-                    touch(a, tq, rq, tl);
-                    if (r == 1) {
-                        const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
-                        if (L && lane == 0) a.live[i] = L;
-                        wlo.push(L != 0 && lane == 0, i);
-                    }
                 }
-                bool tp = false;
-                if (seg != kNoKey) tp = atomicMin(a.best + static_cast<uint64_t>(rp) * kLanes + lane, seg) == kNoKey;
-                touch(a, tp, rp, tl);
+                if (seg != kNoKey) {
+                    offer_min(a, rp, lane, seg);
+                    offered = true;
+                }
             }
             // bridges: one warp per edge
-            for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) edge_lanes(a, i, allmask, r, flat, mj, tl, wlo);
+            for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
+                const bool o = edge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), allmask, r, flat,
+                                          act, wlo, r == 1, true);
+                offered = offered || o;
+            }
         } else {
+            // the worklist of edges live in some MST: 32 entries per warp loaded at
+            // once (index, endpoints, weight, live lanes), then walked two at a time
             const uint32_t cnt = __ldcg(a.ctr + par);
             const uint32_t* in = a.wl + static_cast<uint64_t>(par) * a.E;
-            for (uint32_t t = gw; t < cnt; t += nw) {
-                const uint32_t i = __ldcg(in + t);
-                edge_lanes(a, i, __ldcg(a.live + i), r, flat, mj, tl, wlo);
+            for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
+                const uint32_t m = min(32u, cnt - base);
+                uint32_t my_i = 0, my_u = 0, my_v = 0, my_l = 0;
+                float my_w = 0.0f;
+                if (lane < m) {
+                    my_i = __ldcg(in + base + lane);
+                    my_u = __ldg(a.eu + my_i);
+                    my_v = __ldg(a.ev + my_i);
+                    my_w = __ldg(a.ew + my_i);
+                    my_l = __ldcg(a.live + my_i);
+                }
+                for (uint32_t t = 0; t < m; ++t) {
+                    const uint32_t i = __shfl_sync(0xFFFFFFFFu, my_i, t);
+                    const uint32_t u = __shfl_sync(0xFFFFFFFFu, my_u, t);
+                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, t);
+                    const float w = __shfl_sync(0xFFFFFFFFu, my_w, t);
+                    const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, t);
+                    const bool o = edge_lanes(a, i, u, v, w, l, r, flat, act, wlo, true, false);
+                    offered = offered || o;
+                }
             }
         }
-        tl.flush();
         wlo.flush();
+        if (__any_sync(0xFFFFFFFFu, offered) && lane == 0) a.ctr[5 + par] = 1u;
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-        const uint32_t tcount = __ldcg(a.ctr + 2 + par);
-        if (tcount == 0) break;
-        // ---- phase B
-        for (uint32_t t = gw; t < tcount; t += nw) {
-            const uint32_t c = __ldcg(a.tlist + t);
-            if (lane == 0) a.tflag[c] = 0;
-            unsigned long long* slot = a.best + static_cast<uint64_t>(c) * kLanes + lane;
-            const unsigned long long key = __ldcg(slot);
-            if (key != kNoKey) {
-                *slot = kNoKey;
-                const uint32_t i = static_cast<uint32_t>(key);
-                const uint32_t bit = 1u << lane;
-                if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+        if (__ldcg(a.ctr + 5 + par) == 0u) break;
+        // ---- phase B: every root that took an offer (all nodes in round 0) links
+        // along its best edge; the roots that took one form the next round's list
+        // (a root without an offer has no outgoing live edge: its tree is final)
+        {
+            WarpList rl{s_stage[wib][0], a.rlist + static_cast<uint64_t>(nxt) * a.n, a.ctr + 2 + nxt, 0};
+            const uint32_t rc = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
+            const uint32_t* rin = a.rlist + static_cast<uint64_t>(par) * a.n;
+            for (uint32_t t = gw; t < rc; t += nw) {
+                const uint32_t c = r == 0 ? t : __ldcg(rin + t);
+                unsigned long long* slot = a.best + static_cast<uint64_t>(c) * kLanes + lane;
+                const unsigned long long key = act ? __ldcg(slot) : kNoKey;
+                const bool has = key != kNoKey;
+                const unsigned any = __ballot_sync(0xFFFFFFFFu, has);
+                if (has) {
+                    *slot = kNoKey;
+                    const uint32_t i = static_cast<uint32_t>(key);
+                    const uint32_t bit = 1u << lane;
+                    if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+                }
+                rl.push(any != 0 && lane == 0, c);
             }
+            rl.flush();
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            a.ctr[par] = 0;                  // this round's input, consumed
-            a.ctr[2 + ((r + 1) & 1)] = 0;    // next round's touched count
-        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[par] = 0;  // this round's worklist, consumed
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         // ---- flatten the forests when the next round has enough work to profit
-        const uint32_t next = r == 0 ? a.E : __ldcg(a.ctr + ((r + 1) & 1));
+        const uint32_t next = r == 0 ? a.E : __ldcg(a.ctr + nxt);
         flat = a.flatten_div != 0 && static_cast<uint64_t>(next) * a.flatten_div > a.n;
         if (flat) {
             for (uint32_t v = gw; v < a.n; v += nw) {
@@ -306,6 +355,21 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[4] = static_cast<uint32_t>(r + 1);
+}
+
+/// core[v][j] = core distance of v at mpts[j] (core_dist, include/coresg/knn_graph.hpp:157-163;
+/// +inf for an empty list); lanes >= K hold 0.
+__global__ void k_core32(const float* __restrict__ dists, const uint32_t* __restrict__ counts, uint32_t k,
+                         const uint32_t* __restrict__ mpts, uint32_t K, uint32_t n, float* __restrict__ core) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<uint64_t>(n) * kLanes) return;
+    const uint32_t v = static_cast<uint32_t>(t / kLanes), j = static_cast<uint32_t>(t % kLanes);
+    float x = 0.0f;
+    if (j < K) {
+        const uint32_t c = counts[v], m = mpts[j];
+        x = c == 0 ? __int_as_float(0x7f800000) : dists[static_cast<uint64_t>(v) * k + (m < c ? m : c) - 1];
+    }
+    core[t] = x;
 }
 
 __global__ void k_identity32(uint32_t* __restrict__ parent, uint32_t n) {
@@ -458,7 +522,7 @@ struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
     bool labels = false;
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
-    DevBuf mpts, parent, best, tree, live, wl, tlist, tflag, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins;
+    DevBuf mpts, parent, best, tree, live, wl, rlist, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins;
     cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
     std::vector<uint32_t> host_mpts;
     const void* key_ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -503,8 +567,8 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.tree = p.tree.as<uint32_t>();
     a.live = p.live.as<uint32_t>();
     a.wl = p.wl.as<uint32_t>();
-    a.tlist = p.tlist.as<uint32_t>();
-    a.tflag = p.tflag.as<uint32_t>();
+    a.rlist = p.rlist.as<uint32_t>();
+    a.core = p.core.as<float>();
     a.ctr = p.ctr.as<uint32_t>();
     a.bar = p.bar.as<unsigned>();
     a.status = p.status.as<int>();
@@ -521,10 +585,12 @@ void enqueue_pre(Graph& g, SweepPlan& p) {
     CSB_CUDA(cudaMemsetAsync(p.ctr.p, 0, 64, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.best.p, 0xFF, n * kLanes * 8, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.tree.p, 0, E * 4, c.stream));
-    CSB_CUDA(cudaMemsetAsync(p.tflag.p, 0, n * 4, c.stream));
+
     CSB_CUDA(cudaMemsetAsync(p.bins.p, 0, static_cast<uint64_t>(p.K) * 256 * 8, c.stream));
     k_identity32<<<blocks_for(n * kLanes), kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n);
-    count_launch(c);
+    k_core32<<<blocks_for(n * kLanes), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(), g.k,
+                                                                 p.mpts.as<uint32_t>(), p.K, p.n, p.core.as<float>());
+    count_launch(c, 2);
 }
 
 void enqueue_main(Graph& g, SweepPlan& p) {
@@ -605,7 +671,7 @@ bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
     return ok;
 }
 
-uint64_t kernels_pre() { return 1; }
+uint64_t kernels_pre() { return 2; }
 uint64_t kernels_post(const SweepPlan& p) { return (p.labels ? 4 : 0) + 4; }
 
 /// A plan for the graph's current shape.  `reuse` (a plan that no longer matches)
@@ -648,8 +714,8 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->tree.ensure(E * 4);
         p->live.ensure(E * 4);
         p->wl.ensure(2 * E * 4);
-        p->tlist.ensure(n * 4);
-        p->tflag.ensure(n * 4);
+        p->rlist.ensure(2 * n * 4);
+        p->core.ensure(n * kLanes * 4);
         p->ctr.ensure(64);
         p->bar.ensure(64);
         p->status.ensure(64);
