@@ -72,6 +72,7 @@ _SIGS = {
     "cs_extract_sweep_device": (_i32, [_p, _p, _u32, _p]),
     "cs_sweep_fetch": (_i32, [_p, _u32, _p, _p, _p, _p, _p]),
     "cs_sweep_timing": (_i32, [_p, _p, _p]),
+    "cs_sweep_trace": (_i32, [_p, _p, _u32, _p]),
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
     "cs_mst_noalloc": (_i32, [_p, _p, _p, _u64, _u32, _p, _p, _p, _p, _p, _p]),
@@ -372,6 +373,14 @@ class CoreSG:
         self.ctx.check(lib().cs_sweep_fetch(self.h, index, _ptr(edges), _ptr(lab), C.byref(ne), C.byref(nc),
                                             C.byref(w)))
         return MstResult(edges[:ne.value], None if lab is None else lab[:n], nc.value, w.value)
+
+    def sweep_trace(self) -> np.ndarray:
+        """Per-round profile of the last sweep's first pass: columns phase A ns,
+        phase B ns, flatten ns, edges walked, roots walked, flattened."""
+        out = np.zeros((64, 6), np.uint64)
+        r = C.c_uint32()
+        self.ctx.check(lib().cs_sweep_trace(self.h, _ptr(out), 64, C.byref(r)))
+        return out[: r.value]
 
     def sweep_timing(self):
         """(graph ms, persistent-kernel ms) of the last sweep."""

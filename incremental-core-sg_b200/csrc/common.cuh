@@ -159,6 +159,10 @@ __device__ __forceinline__ uint64_t global_ns() {
 /// when the kernel must stop.
 __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned* gen, int* status,
                                              uint64_t limit_ns) {
+    // every thread first waits for its own writes and reductions to be performed
+    // GPU-wide: an atomic whose result is unused is issued as a reduction and may
+    // otherwise still be in flight when the barrier releases
+    __threadfence();
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {

@@ -52,6 +52,9 @@ constexpr int kThreads = 256;
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
 constexpr int kMaxBlock = 512;
+// per round: globaltimer at the round's start, after phase A, after phase B, after
+// the flatten; edges phase A walked; roots phase B walked
+constexpr int kTraceWords = 6;
 
 inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     uint64_t b = (work + threads - 1) / threads;
@@ -80,6 +83,7 @@ struct SweepArgs {
     unsigned* bar;
     int* status;
     uint64_t limit_ns;
+    unsigned long long* trace;  // [kMaxRounds][kTraceWords] per-round timestamps and sizes
 };
 
 /// find with path halving on forest j of the node-major parent array.
@@ -207,9 +211,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     int r = 0;
     for (; r < kMaxRounds; ++r) {
         const int par = r & 1, nxt = (r + 1) & 1;
+        unsigned long long* tr = a.trace + static_cast<uint64_t>(r) * kTraceWords;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.ctr[2 + nxt] = 0;  // the root list phase B of this round writes
             a.ctr[5 + nxt] = 0;  // next round's offer flag
+            tr[0] = global_ns();
+            tr[3] = 0;
+            tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + par);
+            tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
         }
         WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>(nxt) * a.E, a.ctr + nxt, 0};
         bool offered = false;
@@ -236,7 +245,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                     for (uint32_t t = 0; t < m; t += kUnroll) {
                         uint32_t q[kUnroll], rq[kUnroll];
                         float w[kUnroll], cq[kUnroll];
-                        bool ok[kUnroll], lv[kUnroll];
+                        bool ok[kUnroll];
 #pragma unroll
                         for (int x = 0; x < kUnroll; ++x) {
                             q[x] = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
@@ -250,21 +259,18 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                         for (int x = 0; x < kUnroll; ++x) rq[x] = ok[x] ? root_of(a, q[x], lane, r, flat) : rp;
 #pragma unroll
                         for (int x = 0; x < kUnroll; ++x) {
-                            lv[x] = ok[x] && rp != rq[x];
-                            if (lv[x]) {
+                            const bool lv = ok[x] && rp != rq[x];
+                            if (lv) {
                                 const unsigned long long key = pack_key(max_ref(w[x], max_ref(cp, cq[x])), b + t + x);
                                 seg = key < seg ? key : seg;
                                 offer_min(a, rq[x], lane, key);
                             }
-                        }
-                        if (r == 1) {
-#pragma unroll
-                            for (int x = 0; x < kUnroll; ++x) {
-                                if (t + x < m) {
-                                    const unsigned L = __ballot_sync(0xFFFFFFFFu, lv[x]);
-                                    if (L && lane == 0) a.live[b + t + x] = L;
-                                    wlo.push(L != 0 && lane == 0, b + t + x);
-                                }
+                            // round 1 records the live lanes and builds the worklist; the
+                            // ballot is taken here, next to the value it reads
+                            if (r == 1 && t + x < m) {
+                                const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
+                                if (L && lane == 0) a.live[b + t + x] = L;
+                                wlo.push(L != 0 && lane == 0, b + t + x);
                             }
                         }
                     }
@@ -310,6 +316,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         wlo.flush();
         if (__any_sync(0xFFFFFFFFu, offered) && lane == 0) a.ctr[5 + par] = 1u;
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) tr[1] = global_ns();
         if (__ldcg(a.ctr + 5 + par) == 0u) break;
         // ---- phase B: every root that took an offer (all nodes in round 0) links
         // along its best edge; the roots that took one form the next round's list
@@ -336,6 +343,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[par] = 0;  // this round's worklist, consumed
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) tr[2] = global_ns();
         // ---- flatten the forests when the next round has enough work to profit
         const uint32_t next = r == 0 ? a.E : __ldcg(a.ctr + nxt);
         flat = a.flatten_div != 0 && static_cast<uint64_t>(next) * a.flatten_div > a.n;
@@ -344,6 +352,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                 if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
             }
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+            if (blockIdx.x == 0 && threadIdx.x == 0) tr[3] = global_ns();
         }
     }
     if (r == kMaxRounds) {
@@ -522,7 +531,8 @@ struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
     bool labels = false;
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
-    DevBuf mpts, parent, best, tree, live, wl, rlist, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins;
+    DevBuf mpts, parent, best, tree, live, wl, rlist, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins,
+        trace;
     cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
     std::vector<uint32_t> host_mpts;
     const void* key_ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -568,6 +578,7 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.live = p.live.as<uint32_t>();
     a.wl = p.wl.as<uint32_t>();
     a.rlist = p.rlist.as<uint32_t>();
+    a.trace = p.trace.as<unsigned long long>();
     a.core = p.core.as<float>();
     a.ctr = p.ctr.as<uint32_t>();
     a.bar = p.bar.as<unsigned>();
@@ -717,6 +728,7 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->rlist.ensure(2 * n * 4);
         p->core.ensure(n * kLanes * 4);
         p->ctr.ensure(64);
+        p->trace.ensure(kMaxRounds * kTraceWords * 8);
         p->bar.ensure(64);
         p->status.ensure(64);
         p->cc.ensure(static_cast<uint64_t>(K) * p->ncn * 4 + 64);
@@ -948,6 +960,29 @@ cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint3
         if (out_nedges) *out_nedges = r.nedges;
         if (out_ncomp) *out_ncomp = r.ncomp;
         if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_sweep_trace(cs_graph* gp, uint64_t* out, uint32_t cap_rounds, uint32_t* out_rounds) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        if (!g->plan) fail(CS_ERR_STATE, "cs_sweep_trace: no sweep has run");
+        SweepPlan& p = *g->plan;
+        const uint32_t rounds = std::min<uint32_t>(p.last_rounds, kMaxRounds);
+        std::vector<unsigned long long> t(static_cast<size_t>(kMaxRounds) * kTraceWords);
+        copy_d2h(*g->ctx, t.data(), p.trace.p, t.size() * 8);
+        for (uint32_t r = 0; r < rounds && r < cap_rounds && out; ++r) {
+            const unsigned long long* x = t.data() + static_cast<size_t>(r) * kTraceWords;
+            uint64_t* o = out + static_cast<size_t>(r) * 6;
+            const bool last = r + 1 == rounds;
+            o[0] = x[1] > x[0] ? x[1] - x[0] : 0;                      // phase A
+            o[1] = (!last && x[2] > x[1]) ? x[2] - x[1] : 0;           // phase B
+            o[2] = (!last && x[3] > x[2]) ? x[3] - x[2] : 0;           // flatten
+            o[3] = x[4];
+            o[4] = x[5];
+            o[5] = (!last && x[3] > x[2]) ? 1 : 0;
+        }
+        if (out_rounds) *out_rounds = rounds;
     });
 }
 

@@ -193,3 +193,21 @@ def test_autotune_picks_a_shape(gpu_ctx):
     assert F in (0, 2, 4, 16) and B in (256, 512)
     res = g.all_msts(list(range(1, 9)))
     assert np.array_equal(edge_keys(res[7].edges), z["mst_keys_8"])
+
+
+@pytest.mark.parametrize("shape", [(4, 512), (0xFFFFFFFF, 256), (2, 256)])
+def test_sweep_matches_plain_at_scale(gpu_ctx, shape):
+    """At n = 200,000 (enough Boruvka rounds, warps and blocks for races between
+    phases to show) every batched tree equals the plain path's, edge for edge."""
+    from coresg_b200.datagen import gaussian_mixture
+
+    pts = gaussian_mixture(200_000, 16, 30, (0.2, 1.0), 0.05, seed=77)
+    g = cs.CoreSG(gpu_ctx, 16, 32)
+    g.build(pts)
+    g.set_sweep_shape(*shape)
+    mp = list(range(1, 33))
+    g.sweep_device(mp)
+    for m in (1, 2, 7, 16, 32):
+        plain, swept = g.mst(m), g.sweep_fetch(m - 1)
+        assert swept.edges.tobytes() == plain.edges.tobytes()
+        assert np.array_equal(swept.component, plain.component) and swept.weight == plain.weight
