@@ -172,12 +172,47 @@ __device__ __forceinline__ void offer_min(const SweepArgs& a, uint32_t root, uns
     atomicMin(a.best + static_cast<uint64_t>(root) * kLanes + lane, key);
 }
 
+/// Per-lane two-entry cache of pending offers (root -> smallest key).  Offers to a
+/// root met again soon -- the emitter of consecutive edges, or the few components
+/// of the late rounds, where every edge offers to the same handful of roots -- are
+/// reduced in registers; an atomicMin is issued on eviction and at the flush.
+struct OfferCache {
+    uint32_t r0 = kInvalid, r1 = kInvalid;
+    unsigned long long k0 = kNoKey, k1 = kNoKey;
+    __device__ __forceinline__ void offer(const SweepArgs& a, unsigned lane, uint32_t root, unsigned long long key) {
+        if (root == r0) {
+            k0 = key < k0 ? key : k0;
+            return;
+        }
+        if (root == r1) {  // hit on the second entry: it becomes the first
+            const unsigned long long k = key < k1 ? key : k1;
+            r1 = r0;
+            k1 = k0;
+            r0 = root;
+            k0 = k;
+            return;
+        }
+        if (r1 != kInvalid) offer_min(a, r1, lane, k1);
+        r1 = r0;
+        k1 = k0;
+        r0 = root;
+        k0 = key;
+    }
+    __device__ __forceinline__ void flush(const SweepArgs& a, unsigned lane) {
+        if (r0 != kInvalid) offer_min(a, r0, lane, k0);
+        if (r1 != kInvalid) offer_min(a, r1, lane, k1);
+        r0 = r1 = kInvalid;
+        k0 = k1 = kNoKey;
+    }
+};
+
 /// Phase A for one edge (i, u, v, w) whose live lanes are `lm` (warp-collective).
 /// With `track`, the edge's new live lanes are stored (always when `fresh`: the
 /// word still holds a previous sweep's value) and a live edge is pushed to the next
 /// worklist.  Returns whether this lane offered.
 __device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, uint32_t lm,
-                                           int r, bool flat, bool act, WarpList& wlo, bool track, bool fresh) {
+                                           int r, bool flat, bool act, WarpList& wlo, bool track, bool fresh,
+                                           OfferCache& oc) {
     const unsigned lane = threadIdx.x & 31u;
     bool live = false;
     if (act && ((lm >> lane) & 1u) && u < a.n && v < a.n) {
@@ -187,8 +222,8 @@ __device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint3
         live = ru != rv;
         if (live) {
             const unsigned long long key = pack_key(max_ref(w, max_ref(cu, cv)), i);
-            offer_min(a, ru, lane, key);
-            offer_min(a, rv, lane, key);
+            oc.offer(a, lane, ru, key);
+            oc.offer(a, lane, rv, key);
         }
     }
     if (track) {
@@ -221,6 +256,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
         }
         WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>(nxt) * a.E, a.ctr + nxt, 0};
+        OfferCache oc;
         bool offered = false;
         // ---- phase A
         if (r <= 1) {
@@ -263,7 +299,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                             if (lv) {
                                 const unsigned long long key = pack_key(max_ref(w[x], max_ref(cp, cq[x])), b + t + x);
                                 seg = key < seg ? key : seg;
-                                offer_min(a, rq[x], lane, key);
+                                oc.offer(a, lane, rq[x], key);
                             }
                             // round 1 records the live lanes and builds the worklist; the
                             // ballot is taken here, next to the value it reads
@@ -283,7 +319,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             // bridges: one warp per edge
             for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
                 const bool o = edge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), allmask, r, flat,
-                                          act, wlo, r == 1, true);
+                                          act, wlo, r == 1, true, oc);
                 offered = offered || o;
             }
         } else {
@@ -308,11 +344,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                     const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, t);
                     const float w = __shfl_sync(0xFFFFFFFFu, my_w, t);
                     const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, t);
-                    const bool o = edge_lanes(a, i, u, v, w, l, r, flat, act, wlo, true, false);
+                    const bool o = edge_lanes(a, i, u, v, w, l, r, flat, act, wlo, true, false, oc);
                     offered = offered || o;
                 }
             }
         }
+        oc.flush(a, lane);
         wlo.flush();
         if (__any_sync(0xFFFFFFFFu, offered) && lane == 0) a.ctr[5 + par] = 1u;
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
