@@ -244,9 +244,10 @@ cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32
 /* Device times of the last sweep: the whole captured sequence and the persistent
  * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
 cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
-/* Per-round profile of the first pass of the last sweep, 6 words per Boruvka round:
+/* Per-round profile of the first pass of the last sweep, 7 words per Boruvka round:
  * device ns of phase A (offers), phase B (links) and the forest flatten (0 when the
- * round did not flatten), edges phase A walked, roots phase B walked, flattened (0/1).
+ * round did not flatten), edges phase A walked, roots phase B walked, flattened (0/1),
+ * live (edge, MST) pairs phase A found.
  * Writes min(rounds, cap_rounds) rows; *out_rounds = rounds (the last round ends after
  * its phase A). */
 cs_status cs_sweep_trace(cs_graph* g, uint64_t* out, uint32_t cap_rounds, uint32_t* out_rounds);

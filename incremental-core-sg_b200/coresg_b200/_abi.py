@@ -376,8 +376,9 @@ class CoreSG:
 
     def sweep_trace(self) -> np.ndarray:
         """Per-round profile of the last sweep's first pass: columns phase A ns,
-        phase B ns, flatten ns, edges walked, roots walked, flattened."""
-        out = np.zeros((64, 6), np.uint64)
+        phase B ns, flatten ns, edges walked, roots walked, flattened, live
+        (edge, MST) pairs."""
+        out = np.zeros((64, 7), np.uint64)
         r = C.c_uint32()
         self.ctx.check(lib().cs_sweep_trace(self.h, _ptr(out), 64, C.byref(r)))
         return out[: r.value]

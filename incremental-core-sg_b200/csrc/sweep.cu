@@ -53,8 +53,9 @@ constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
 constexpr int kMaxBlock = 512;
 // per round: globaltimer at the round's start, after phase A, after phase B, after
-// the flatten; edges phase A walked; roots phase B walked
-constexpr int kTraceWords = 6;
+// the flatten; edges phase A walked; roots phase B walked; live (edge, MST) pairs
+// phase A found
+constexpr int kTraceWords = 7;
 
 inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     uint64_t b = (work + threads - 1) / threads;
@@ -254,10 +255,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             tr[3] = 0;
             tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + par);
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
+            tr[6] = 0;
         }
         WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>(nxt) * a.E, a.ctr + nxt, 0};
         OfferCache oc;
         bool offered = false;
+        uint32_t live_pairs = 0;
         // ---- phase A
         if (r <= 1) {
             // k-NN edges, node by node over the emitted segments: 32 edges of a
@@ -296,6 +299,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
 #pragma unroll
                         for (int x = 0; x < kUnroll; ++x) {
                             const bool lv = ok[x] && rp != rq[x];
+                            live_pairs += lv ? 1u : 0u;
                             if (lv) {
                                 const unsigned long long key = pack_key(max_ref(w[x], max_ref(cp, cq[x])), b + t + x);
                                 seg = key < seg ? key : seg;
@@ -338,19 +342,58 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                     my_w = __ldg(a.ew + my_i);
                     my_l = __ldcg(a.live + my_i);
                 }
-                for (uint32_t t = 0; t < m; ++t) {
-                    const uint32_t i = __shfl_sync(0xFFFFFFFFu, my_i, t);
-                    const uint32_t u = __shfl_sync(0xFFFFFFFFu, my_u, t);
-                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, t);
-                    const float w = __shfl_sync(0xFFFFFFFFu, my_w, t);
-                    const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, t);
-                    const bool o = edge_lanes(a, i, u, v, w, l, r, flat, act, wlo, true, false, oc);
-                    offered = offered || o;
+                for (uint32_t t = 0; t < m; t += kUnroll) {
+                    // kUnroll edges at a time: their core and root loads are issued
+                    // together, then each edge offers and records its live lanes
+                    uint32_t ei[kUnroll], eu[kUnroll], ev[kUnroll], el[kUnroll], ru[kUnroll], rv[kUnroll];
+                    float ew[kUnroll], cu[kUnroll], cv[kUnroll];
+                    bool ok[kUnroll];
+#pragma unroll
+                    for (int x = 0; x < kUnroll; ++x) {
+                        const uint32_t src = (t + x) & 31u;
+                        ei[x] = __shfl_sync(0xFFFFFFFFu, my_i, src);
+                        eu[x] = __shfl_sync(0xFFFFFFFFu, my_u, src);
+                        ev[x] = __shfl_sync(0xFFFFFFFFu, my_v, src);
+                        ew[x] = __shfl_sync(0xFFFFFFFFu, my_w, src);
+                        el[x] = __shfl_sync(0xFFFFFFFFu, my_l, src);
+                        ok[x] = act && t + x < m && ((el[x] >> lane) & 1u) && eu[x] < a.n && ev[x] < a.n;
+                    }
+#pragma unroll
+                    for (int x = 0; x < kUnroll; ++x) {
+                        cu[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(eu[x]) * kLanes + lane) : 0.0f;
+                        cv[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(ev[x]) * kLanes + lane) : 0.0f;
+                    }
+#pragma unroll
+                    for (int x = 0; x < kUnroll; ++x) {
+                        ru[x] = ok[x] ? root_of(a, eu[x], lane, r, flat) : 0u;
+                        rv[x] = ok[x] ? root_of(a, ev[x], lane, r, flat) : 0u;
+                    }
+#pragma unroll
+                    for (int x = 0; x < kUnroll; ++x) {
+                        const bool lv = ok[x] && ru[x] != rv[x];
+                        live_pairs += lv ? 1u : 0u;
+                        if (lv) {
+                            const unsigned long long key = pack_key(max_ref(ew[x], max_ref(cu[x], cv[x])), ei[x]);
+                            oc.offer(a, lane, ru[x], key);
+                            oc.offer(a, lane, rv[x], key);
+                            offered = true;
+                        }
+                        if (t + x < m) {  // ballot next to the value it reads
+                            const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
+                            if (L && L != el[x] && lane == 0) a.live[ei[x]] = L;
+                            wlo.push(L != 0 && lane == 0, ei[x]);
+                        }
+                    }
                 }
             }
         }
         oc.flush(a, lane);
         wlo.flush();
+        {
+            unsigned long long lp = live_pairs;
+            for (int o = 16; o > 0; o >>= 1) lp += __shfl_xor_sync(0xFFFFFFFFu, lp, o);
+            if (lane == 0 && lp) atomicAdd(tr + 6, lp);
+        }
         if (__any_sync(0xFFFFFFFFu, offered) && lane == 0) a.ctr[5 + par] = 1u;
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[1] = global_ns();
@@ -1010,7 +1053,7 @@ cs_status cs_sweep_trace(cs_graph* gp, uint64_t* out, uint32_t cap_rounds, uint3
         copy_d2h(*g->ctx, t.data(), p.trace.p, t.size() * 8);
         for (uint32_t r = 0; r < rounds && r < cap_rounds && out; ++r) {
             const unsigned long long* x = t.data() + static_cast<size_t>(r) * kTraceWords;
-            uint64_t* o = out + static_cast<size_t>(r) * 6;
+            uint64_t* o = out + static_cast<size_t>(r) * 7;
             const bool last = r + 1 == rounds;
             o[0] = x[1] > x[0] ? x[1] - x[0] : 0;                      // phase A
             o[1] = (!last && x[2] > x[1]) ? x[2] - x[1] : 0;           // phase B
@@ -1018,6 +1061,7 @@ cs_status cs_sweep_trace(cs_graph* gp, uint64_t* out, uint32_t cap_rounds, uint3
             o[3] = x[4];
             o[4] = x[5];
             o[5] = (!last && x[3] > x[2]) ? 1 : 0;
+            o[6] = x[6];
         }
         if (out_rounds) *out_rounds = rounds;
     });
