@@ -187,6 +187,22 @@ void cs_insert_defaults(cs_insert_params* p);
  * and are topped up with random points of the batch, src/incremental_knn.cpp:808-840),
  * then the restricted refinement.
  * out_active, out_updates may be NULL. */
+/* Stages of the last cs_insert on a graph (IncrementalKnnStats,
+ * include/coresg/incremental_knn.hpp:270-300): device milliseconds of the reverse
+ * index, the seeding search + seed application, the instance descent, the
+ * restricted refinement and the finalisation, and host milliseconds of the bridge
+ * re-selection and of the whole call. */
+typedef struct {
+    uint64_t new_points;
+    uint64_t instance_nodes;  /* new points + context */
+    uint64_t refine_nodes;
+    uint64_t updates;
+    uint32_t rounds;          /* descent rounds run (instance + refinement) */
+    uint32_t reserved0;
+    double reverse_ms, search_ms, instance_ms, refine_ms, finish_ms, bridges_ms, total_ms;
+} cs_insert_stats;
+cs_status cs_insert_stats_get(cs_graph* g, cs_insert_stats* out);
+
 cs_status cs_insert(cs_graph* g, const float* rows, uint64_t count, uint32_t row_stride,
                     const cs_insert_params* params, uint64_t* out_active, uint64_t* out_updates);
 

@@ -64,6 +64,7 @@ _SIGS = {
     "cs_select_bridges": (_i32, [_p, _p, _p, _p, _p]),
     "cs_insert_defaults": (None, [_p]),
     "cs_insert": (_i32, [_p, _p, _u64, _u32, _p, _p, _p]),
+    "cs_insert_stats_get": (_i32, [_p, _p]),
     "cs_get_selected": (_i32, [_p, _p, _u64, _p]),
     "cs_core_distances": (_i32, [_p, _u32, _p]),
     "cs_edges": (_i32, [_p, _u32, _p, _u64, _p]),
@@ -181,6 +182,14 @@ class InsertParams(C.Structure):
                 ("context_per_new", C.c_double), ("owned_warm_fraction", C.c_double), ("refine_per_new", C.c_double),
                 ("refine_max_fraction", C.c_double), ("delta", C.c_double), ("max_expand", C.c_uint32),
                 ("reverse_cap", C.c_uint32), ("seed", C.c_uint64), ("reselect_bridges", C.c_int32)]
+
+
+class InsertStats(C.Structure):
+    _fields_ = [("new_points", C.c_uint64), ("instance_nodes", C.c_uint64), ("refine_nodes", C.c_uint64),
+                ("updates", C.c_uint64), ("rounds", C.c_uint32), ("reserved0", C.c_uint32),
+                ("reverse_ms", C.c_double), ("search_ms", C.c_double), ("instance_ms", C.c_double),
+                ("refine_ms", C.c_double), ("finish_ms", C.c_double), ("bridges_ms", C.c_double),
+                ("total_ms", C.c_double)]
 
 
 class MstResult:
@@ -312,6 +321,12 @@ class CoreSG:
         self.ctx.check(lib().cs_insert(self.h, _ptr(rows), rows.shape[0], rows.shape[1], C.byref(p), C.byref(act),
                                        C.byref(upd)))
         return dict(active=act.value, updates=upd.value)
+
+    def insert_stats(self) -> dict:
+        """Stages of the last insert (cs_insert_stats_get)."""
+        x = InsertStats()
+        self.ctx.check(lib().cs_insert_stats_get(self.h, C.byref(x)))
+        return {name: getattr(x, name) for name, _ in InsertStats._fields_ if name != "reserved0"}
 
     def build(self, rows: np.ndarray, sample=16, iters=10, delta=0.001, seed=42):
         """CoreSG::build: points, NN-Descent, bridges (src/coresg.cpp:260-323)."""

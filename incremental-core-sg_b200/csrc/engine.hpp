@@ -123,6 +123,9 @@ struct Graph {
     DevBuf insert_scratch[12];
     DevBuf bridge_scratch[23];
 
+    // Stages of the last cs_insert.
+    cs_insert_stats last_insert{};
+
     // Hubness selection of the last cs_select_bridges.
     std::vector<uint32_t> selected;
 
@@ -185,6 +188,7 @@ struct InsertStats {
     uint64_t active = 0, updates = 0;
     uint32_t rounds = 0;
     double search_ms = 0.0, refine_ms = 0.0;
+    cs_insert_stats detail{};
 };
 void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride, const cs_insert_params& p,
                 InsertStats* st);

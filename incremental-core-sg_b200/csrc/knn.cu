@@ -25,6 +25,7 @@
 // with an IEEE sqrt at the end, so every stored distance equals the reference's
 // metric_distance for that pair bit for bit.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -520,7 +521,11 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
         unsigned long long best = kNoKey;
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-            if (key[i] != kNoKey && !(pay[i] & 1u) && key[i] < best) best = key[i];
+            // only the ef best may be expanded: the search ends when the nearest
+            // unexpanded candidate is behind them (the reference's beam rule)
+            if (key[i] != kNoKey && !(pay[i] & 1u) && static_cast<uint32_t>(i) * 32u + lane < width &&
+                key[i] < best)
+                best = key[i];
         }
         for (int o = 16; o > 0; o >>= 1) {
             const unsigned long long x = __shfl_xor_sync(0xFFFFFFFFu, best, o);
@@ -544,6 +549,11 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
             bool ok = nb < n_base;
             unsigned long long ck = kNoKey;
             if (ok) ck = make_key(l2sqr_ref(qrow, pts + static_cast<uint64_t>(nb) * stride, stride), nb);
+            // a candidate behind the pool's last key cannot enter: most expansions
+            // near convergence bring none, and skip the dedupe and the sort
+            const unsigned long long worst = __shfl_sync(0xFFFFFFFFu, key[1], 31);
+            ok = ok && ck < worst;
+            if (!__any_sync(0xFFFFFFFFu, ok)) continue;
             for (int s2 = 0; s2 < 32; ++s2) {
 #pragma unroll
                 for (int i = 0; i < 2; ++i) {
@@ -897,10 +907,10 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     const uint32_t first_new = static_cast<uint32_t>(g.n);
     graph_set_points(g, rows, count, row_stride, true);
     const uint32_t n = static_cast<uint32_t>(g.n), k = g.k, nn = static_cast<uint32_t>(count);
-    cudaEvent_t e0, e1, e2;
-    CSB_CUDA(cudaEventCreate(&e0));
-    CSB_CUDA(cudaEventCreate(&e1));
-    CSB_CUDA(cudaEventCreate(&e2));
+    // stage events: start, reverse index, search + seeds, instance, refinement, end
+    cudaEvent_t ev[6];
+    for (auto& e : ev) CSB_CUDA(cudaEventCreate(&e));
+    cudaEvent_t &e0 = ev[0], &e1 = ev[2], &e2 = ev[5];
     Descent d(g, p.sample);
     CSB_CUDA(cudaEventRecord(e0, c.stream));
     // seeding search over the base graph (ef = 2k results, at most the 64-entry
@@ -931,16 +941,18 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
                                                                first_new, rev_keys.as<unsigned long long>(),
                                                                rev_deg.as<uint32_t>());
         count_launch(c);
-        // targets fit below bit end_bit; a valid key's source is < 2^32 - 1, so the
-        // invalid key ~0 still sorts after every valid one over bits [0, end_bit)
+        // targets fit below bit end_bit; the invalid key ~0 has every target bit set,
+        // above any valid target (< first_new < 2^(end_bit-32)), so it sorts last
         int end_bit = 33;
         while (end_bit < 64 && (1ull << (end_bit - 32)) <= first_new) ++end_bit;
         cub::DoubleBuffer<unsigned long long> db(rev_keys.as<unsigned long long>(), rev_alt.as<unsigned long long>());
         size_t tmp_bytes = 0;
-        CSB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(nk), 0, end_bit, c.stream));
+        // keys are written in source order and the radix sort is stable, so sorting
+        // the target bits alone leaves each node's reverse list ascending by source
+        CSB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(nk), 32, end_bit, c.stream));
         sort_tmp.ensure(tmp_bytes + 16);
-        CSB_CUDA(cub::DeviceRadixSort::SortKeys(sort_tmp.p, tmp_bytes, db, static_cast<int>(nk), 0, end_bit, c.stream));
-        count_launch(c, static_cast<uint64_t>((end_bit + 7) / 8) + 1);  // histogram + one per digit
+        CSB_CUDA(cub::DeviceRadixSort::SortKeys(sort_tmp.p, tmp_bytes, db, static_cast<int>(nk), 32, end_bit, c.stream));
+        count_launch(c, static_cast<uint64_t>((end_bit - 32 + 7) / 8) + 1);  // histogram + one per digit
         if (db.Current() != rev_keys.as<unsigned long long>()) {
             std::swap(rev_keys.p, rev_alt.p);
             std::swap(rev_keys.bytes, rev_alt.bytes);
@@ -948,6 +960,7 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
         scan_u32(c, rev_deg.as<uint32_t>(), rev_off.as<uint32_t>(), first_new);
         check_launch(c, "insert reverse index");
     }
+    CSB_CUDA(cudaEventRecord(ev[1], c.stream));
     const uint32_t max_expand = p.max_expand ? p.max_expand : 8 * k;
     const size_t qsmem = static_cast<size_t>(kWarps) * g.stride * 4;
     k_search<<<(nn + kWarps - 1) / kWarps, kThreads, qsmem, c.stream>>>(
@@ -1011,31 +1024,46 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
         launch_merge(c, g, d.s, nullptr);
         check_launch(c, "insert seed merge");
     }
+    CSB_CUDA(cudaEventRecord(ev[3], c.stream));
+    const uint32_t n_instance = n_active;
     // the restricted refinement (refine_per_new, refine_max_fraction)
     uint64_t cap = n;
     if (p.refine_max_fraction > 0.0 && p.refine_max_fraction < 1.0) cap = static_cast<uint64_t>(p.refine_max_fraction * n);
     if (p.refine_per_new > 0.0) cap = std::min<uint64_t>(cap, static_cast<uint64_t>(p.refine_per_new * nn));
+    uint32_t n_ref = 0;
     if (p.refine_iters) {
-        const uint32_t n_ref = active_set(cap, false);
+        n_ref = active_set(cap, false);
         upd += d.rounds(active.as<uint32_t>(), n_ref, p.refine_iters, p.delta, &r2);
         n_active = std::max(n_active, n_ref);
     }
     rounds += r2;
+    CSB_CUDA(cudaEventRecord(ev[4], c.stream));
     d.finish();
     CSB_CUDA(cudaEventRecord(e2, c.stream));
     CSB_CUDA(cudaEventSynchronize(e2));
+    float ms[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < 5; ++i) CSB_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
     float ms_search = 0.0f, ms_refine = 0.0f;
     CSB_CUDA(cudaEventElapsedTime(&ms_search, e0, e1));
     CSB_CUDA(cudaEventElapsedTime(&ms_refine, e1, e2));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
+    for (auto& e : ev) cudaEventDestroy(e);
     if (st) {
         st->active = n_active;
         st->updates = upd;
         st->rounds = rounds;
         st->search_ms = ms_search;
         st->refine_ms = ms_refine;
+        cs_insert_stats& x = st->detail;
+        x.new_points = nn;
+        x.instance_nodes = n_instance;
+        x.refine_nodes = n_ref;
+        x.updates = upd;
+        x.rounds = rounds;
+        x.reverse_ms = ms[0];
+        x.search_ms = ms[1];
+        x.instance_ms = ms[2];
+        x.refine_ms = ms[3];
+        x.finish_ms = ms[4];
     }
 }
 
@@ -1100,6 +1128,14 @@ void cs_insert_defaults(cs_insert_params* p) {
     p->reselect_bridges = 1;
 }
 
+cs_status cs_insert_stats_get(cs_graph* gp, cs_insert_stats* out) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(out != nullptr, "cs_insert_stats_get: null out");
+        *out = g->last_insert;
+    });
+}
+
 cs_status cs_insert(cs_graph* gp, const float* rows, uint64_t count, uint32_t row_stride,
                     const cs_insert_params* params, uint64_t* out_active, uint64_t* out_updates) {
     Graph* g = reinterpret_cast<Graph*>(gp);
@@ -1109,8 +1145,14 @@ cs_status cs_insert(cs_graph* gp, const float* rows, uint64_t count, uint32_t ro
         cs_insert_defaults(&p);
         if (params) p = *params;
         InsertStats st;
+        const auto t0 = std::chrono::steady_clock::now();
         knn_insert(*g, rows, count, row_stride, p, &st);
+        const auto t1 = std::chrono::steady_clock::now();
         if (p.reselect_bridges && count) select_bridges(*g, nullptr, nullptr, nullptr, nullptr);
+        const auto t2 = std::chrono::steady_clock::now();
+        st.detail.bridges_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        st.detail.total_ms = std::chrono::duration<double, std::milli>(t2 - t0).count();
+        g->last_insert = st.detail;
         if (out_active) *out_active = st.active;
         if (out_updates) *out_updates = st.updates;
     });

@@ -127,36 +127,22 @@ __device__ __forceinline__ bool unite32(uint32_t* parent, uint32_t a, uint32_t b
     return false;
 }
 
-/// Per-warp list buffer in shared memory: appends are staged and flushed to the
-/// global list 32 at a time with one atomicAdd on the list's counter.
-struct WarpList {
-    uint32_t* stage;  // 32 entries of this warp's shared memory
-    uint32_t* list;
-    uint32_t* counter;
-    uint32_t n;  // warp-uniform fill
-    __device__ __forceinline__ void flush() {
-        if (n == 0) return;
-        __syncwarp();
-        const unsigned lane = threadIdx.x & 31u;
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(counter, n);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (lane < n) list[base + lane] = stage[lane];
-        __syncwarp();
-        n = 0;
-    }
-    /// warp-collective: every lane with `pred` appends `v`
-    __device__ __forceinline__ void push(bool pred, uint32_t v) {
-        const unsigned m = __ballot_sync(0xFFFFFFFFu, pred);
-        if (!m) return;
-        const uint32_t c = __popc(m);
-        if (n + c > 32) flush();
-        const unsigned lane = threadIdx.x & 31u;
-        if (pred) stage[n + __popc(m & ((1u << lane) - 1u))] = v;
-        __syncwarp();
-        n += c;
-    }
-};
+/// Append the entries of a warp's chunk whose bits are set in the warp-uniform
+/// `mask` (bit t: the entry held by lane t) to list `which` of the double buffer
+/// `lists` (cap entries each; counters[which] counts it): one atomicAdd reserves the
+/// exact count, then every marked lane writes its own entry, in lane order.
+__device__ __forceinline__ void chunk_append(uint32_t* lists, uint32_t* counters, int which, uint32_t cap,
+                                             uint32_t mask, uint32_t mine) {
+    if (!mask) return;
+    // the list and its counter are derived here, next to their use
+    uint32_t* const list = lists + static_cast<uint64_t>(which) * cap;
+    uint32_t* const counter = counters + which;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if ((mask >> lane) & 1u) list[base + __popc(mask & ((1u << lane) - 1u))] = mine;
+}
 
 constexpr int kUnroll = 4;  // edges in flight per warp in the node-segment rounds
 
@@ -209,11 +195,10 @@ struct OfferCache {
 
 /// Phase A for one edge (i, u, v, w) whose live lanes are `lm` (warp-collective).
 /// With `track`, the edge's new live lanes are stored (always when `fresh`: the
-/// word still holds a previous sweep's value) and a live edge is pushed to the next
+/// word still holds a previous sweep's value) and a live edge is appended to the next
 /// worklist.  Returns whether this lane offered.
 __device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, uint32_t lm,
-                                           int r, bool flat, bool act, WarpList& wlo, bool track, bool fresh,
-                                           OfferCache& oc) {
+                                           int r, bool flat, bool act, bool track, bool fresh, OfferCache& oc) {
     const unsigned lane = threadIdx.x & 31u;
     bool live = false;
     if (act && ((lm >> lane) & 1u) && u < a.n && v < a.n) {
@@ -230,15 +215,16 @@ __device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint3
     if (track) {
         const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
         if (L && (fresh || L != lm) && lane == 0) a.live[i] = L;
-        wlo.push(L != 0 && lane == 0, i);
+        if (L && lane == 0) {
+            const int which = (r + 1) & 1;
+            a.wl[static_cast<uint64_t>(which) * a.E + atomicAdd(a.ctr + which, 1u)] = i;
+        }
     }
     return live;
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
-    __shared__ uint32_t s_stage[kMaxBlock / 32][2][32];
     const unsigned lane = threadIdx.x & 31u;
-    const unsigned wib = threadIdx.x >> 5;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const bool act = lane < a.K;
@@ -257,7 +243,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
             tr[6] = 0;
         }
-        WarpList wlo{s_stage[wib][1], a.wl + static_cast<uint64_t>(nxt) * a.E, a.ctr + nxt, 0};
         OfferCache oc;
         bool offered = false;
         uint32_t live_pairs = 0;
@@ -274,6 +259,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                 unsigned long long seg = kNoKey;
                 for (uint32_t b = beg; b < end; b += 32) {
                     const uint32_t m = min(32u, end - b);
+                    uint32_t pmask = 0;  // round 1: edges of this chunk that stay live
                     uint32_t my_q = 0;
                     float my_w = 0.0f;
                     if (lane < m) {
@@ -310,10 +296,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                             if (r == 1 && t + x < m) {
                                 const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
                                 if (L && lane == 0) a.live[b + t + x] = L;
-                                wlo.push(L != 0 && lane == 0, b + t + x);
+                                if (L) pmask |= 1u << (t + x);
                             }
                         }
                     }
+                    if (r == 1) chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, b + lane);
                 }
                 if (seg != kNoKey) {
                     offer_min(a, rp, lane, seg);
@@ -323,7 +310,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             // bridges: one warp per edge
             for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
                 const bool o = edge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), allmask, r, flat,
-                                          act, wlo, r == 1, true, oc);
+                                          act, r == 1, true, oc);
                 offered = offered || o;
             }
         } else {
@@ -342,6 +329,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                     my_w = __ldg(a.ew + my_i);
                     my_l = __ldcg(a.live + my_i);
                 }
+                uint32_t pmask = 0;  // entries of this chunk that stay live
                 for (uint32_t t = 0; t < m; t += kUnroll) {
                     // kUnroll edges at a time: their core and root loads are issued
                     // together, then each edge offers and records its live lanes
@@ -381,14 +369,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                         if (t + x < m) {  // ballot next to the value it reads
                             const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
                             if (L && L != el[x] && lane == 0) a.live[ei[x]] = L;
-                            wlo.push(L != 0 && lane == 0, ei[x]);
+                            if (L) pmask |= 1u << (t + x);
                         }
                     }
                 }
+                chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, my_i);
             }
         }
         oc.flush(a, lane);
-        wlo.flush();
         {
             unsigned long long lp = live_pairs;
             for (int o = 16; o > 0; o >>= 1) lp += __shfl_xor_sync(0xFFFFFFFFu, lp, o);
@@ -402,24 +390,27 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         // along its best edge; the roots that took one form the next round's list
         // (a root without an offer has no outgoing live edge: its tree is final)
         {
-            WarpList rl{s_stage[wib][0], a.rlist + static_cast<uint64_t>(nxt) * a.n, a.ctr + 2 + nxt, 0};
             const uint32_t rc = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
             const uint32_t* rin = a.rlist + static_cast<uint64_t>(par) * a.n;
-            for (uint32_t t = gw; t < rc; t += nw) {
-                const uint32_t c = r == 0 ? t : __ldcg(rin + t);
-                unsigned long long* slot = a.best + static_cast<uint64_t>(c) * kLanes + lane;
-                const unsigned long long key = act ? __ldcg(slot) : kNoKey;
-                const bool has = key != kNoKey;
-                const unsigned any = __ballot_sync(0xFFFFFFFFu, has);
-                if (has) {
-                    *slot = kNoKey;
-                    const uint32_t i = static_cast<uint32_t>(key);
-                    const uint32_t bit = 1u << lane;
-                    if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+            for (uint32_t base = gw * 32u; base < rc; base += nw * 32u) {
+                const uint32_t m = min(32u, rc - base);
+                const uint32_t my_c = lane < m ? (r == 0 ? base + lane : __ldcg(rin + base + lane)) : 0u;
+                uint32_t keep = 0;  // roots of this chunk that took an offer
+                for (uint32_t t = 0; t < m; ++t) {
+                    const uint32_t c = __shfl_sync(0xFFFFFFFFu, my_c, t);
+                    unsigned long long* slot = a.best + static_cast<uint64_t>(c) * kLanes + lane;
+                    const unsigned long long key = act ? __ldcg(slot) : kNoKey;
+                    const bool has = key != kNoKey;
+                    if (__ballot_sync(0xFFFFFFFFu, has)) keep |= 1u << t;
+                    if (has) {
+                        *slot = kNoKey;
+                        const uint32_t i = static_cast<uint32_t>(key);
+                        const uint32_t bit = 1u << lane;
+                        if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+                    }
                 }
-                rl.push(any != 0 && lane == 0, c);
+                chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
             }
-            rl.flush();
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[par] = 0;  // this round's worklist, consumed
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
