@@ -61,7 +61,7 @@ struct Slot {
     DevBuf edges;   // cs_edge [n-1]
     DevBuf labels;  // u32 [n]
     DevBuf meta;    // u64 [kMetaWords]
-    uint64_t n = 0; // node count the slot holds
+    uint64_t n = 0; // nodes the slot can hold
     size_t bytes() const { return edges.bytes + labels.bytes + meta.bytes; }
 };
 
@@ -126,34 +126,37 @@ struct Server {
     /// A slot for `n` nodes, or null when none is free and memory does not admit a
     /// new one (the caller waits for the batches in flight).  Under mu.
     Slot* try_slot(uint64_t n) {
+        // a free slot that holds n nodes is reused as it is: slots are sized with a
+        // quarter of headroom, so a graph that grows by inserts keeps its slots
         for (size_t i = 0; i < free_slots.size(); ++i) {
-            if (free_slots[i]->n == n) {
+            if (free_slots[i]->n >= n) {
                 Slot* s = free_slots[i];
                 free_slots.erase(free_slots.begin() + static_cast<long>(i));
                 return s;
             }
         }
-        // slots of an older graph size are released before new ones are made
+        // slots too small for the grown graph are released before new ones are made
         for (Slot* s : free_slots) {
             all_slots.erase(std::find(all_slots.begin(), all_slots.end(), s));
             delete s;
         }
         free_slots.clear();
         if (all_slots.size() >= cfg.max_slots) return nullptr;
+        const uint64_t cap = n + n / 4;
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
-        const size_t need = slot_bytes_for(n);
+        const size_t need = slot_bytes_for(cap);
         if (free_b < need + cfg.reserve_bytes) return nullptr;
         Slot* s = new Slot;
         try {
-            s->edges.ensure(std::max<uint64_t>(n ? n - 1 : 0, 1) * sizeof(cs_edge));
-            s->labels.ensure(std::max<uint64_t>(n, 1) * 4);
+            s->edges.ensure(std::max<uint64_t>(cap ? cap - 1 : 0, 1) * sizeof(cs_edge));
+            s->labels.ensure(std::max<uint64_t>(cap, 1) * 4);
             s->meta.ensure(kMetaWords * 8);
         } catch (const Error&) {
             delete s;
             return nullptr;
         }
-        s->n = n;
+        s->n = cap;
         all_slots.push_back(s);
         st.slots = all_slots.size();
         st.slot_bytes = s->bytes();
