@@ -261,17 +261,18 @@ cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32
  * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
 cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
 /* Per-round profile of the first pass of the last sweep, 7 words per Boruvka round:
- * device ns of phase A (offers), phase B (links) and the forest flatten (0 when the
- * round did not flatten), edges phase A walked, roots phase B walked, flattened (0/1),
- * live (edge, MST) pairs phase A found.
+ * device ns of phase A (offers), phase B (links) and the forest flatten, edges phase A
+ * walked, roots phase B walked, every node flattened (0/1), live (edge, MST) pairs
+ * phase A found.
  * Writes min(rounds, cap_rounds) rows; *out_rounds = rounds (the last round ends after
  * its phase A). */
 cs_status cs_sweep_trace(cs_graph* g, uint64_t* out, uint32_t cap_rounds, uint32_t* out_rounds);
 
-/* Sweep tuning knobs.  flatten_div: the union-find forests are flattened between
- * Boruvka rounds when the next round's worklist exceeds n / flatten_div
- * (0xFFFFFFFF: never); block_threads: 128, 256 or 512.  0 picks the value cached by
- * cs_autotune_sweep for this (n, |E|, K, SM count), else the defaults (4, 512). */
+/* Sweep tuning knobs.  flatten_div: after every Boruvka round the roots that were
+ * linked point at their final roots; from round 2 on, every node is flattened too when
+ * the round's live (edge, MST) pairs exceed 32 n / flatten_div (0xFFFFFFFF: never);
+ * block_threads: 128, 256 or 512.  0 picks the value cached by cs_autotune_sweep for
+ * this (n, |E|, K, SM count), else the defaults (never, 512). */
 cs_status cs_set_sweep_shape(cs_graph* g, uint32_t flatten_div, uint32_t block_threads);
 /* Project-written autotuner: times every (block, flatten_div) pair on the resident
  * graph and caches the fastest for later sweeps of this shape. */

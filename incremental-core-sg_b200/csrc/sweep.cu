@@ -17,10 +17,12 @@
 //   * rounds 0 and 1 walk each node's emitted segment (the node-major enumeration of
 //     src/knn_graph.cpp:132-200), so the emitter-side atomicMin of every lane is
 //     aggregated over the segment in registers and issued once;
-//   * between rounds the union-find forests are flattened (parent[v][j] = root), so
-//     the next round's root lookups are single coalesced loads;
-//   * worklist and touched-root appends are buffered per warp in shared memory and
-//     flushed 32 at a time (one atomicAdd per flush);
+//   * between rounds the roots that phase B may have linked are pointed at their
+//     final roots, so a root lookup takes at most two loads; while the live (edge,
+//     MST) pairs outnumber the nodes enough, every node is flattened as well
+//     (parent[v][j] = root) and a lookup is one coalesced load;
+//   * worklist and root-list appends go 32 entries of a warp at a time (one
+//     atomicAdd per chunk);
 //   * the phases are separated by a bounded grid barrier of a cooperative launch, and
 //     the state reset, the persistent kernel and the finishing kernels (labels, tree
 //     compaction, exact weights) are each captured once into a CUDA graph.
@@ -54,8 +56,8 @@ constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
 constexpr int kMaxBlock = 512;
 // per round: globaltimer at the round's start, after phase A, after phase B, after
 // the flatten; edges phase A walked; roots phase B walked; live (edge, MST) pairs
-// phase A found
-constexpr int kTraceWords = 7;
+// phase A found; whether every node was flattened
+constexpr int kTraceWords = 8;
 
 inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     uint64_t b = (work + threads - 1) / threads;
@@ -64,7 +66,7 @@ inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
 
 struct SweepArgs {
     uint32_t n, E, e_knn, K, k;
-    uint32_t flatten_div;  // flatten when the next worklist exceeds n / flatten_div (0: never)
+    uint32_t flatten_div;  // flatten every node when live pairs exceed 32 n / flatten_div (0: never)
     const uint32_t* eu;
     const uint32_t* ev;
     const float* ew;
@@ -78,9 +80,10 @@ struct SweepArgs {
     uint32_t* live;            // [E] bit j: edge live in MST j
     uint32_t* wl;              // [2][E]
     uint32_t* rlist;           // [2][n] roots that took an offer in the previous round
+    uint32_t* fl;              // [n] frozen root list: roots as of the last full flatten
     const float* core;         // [n][32] core distance of v at mpts[j]
     uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] root-list counts; [4] rounds;
-                               // [5],[6] "some edge offered" flags
+                               // [5],[6] "some edge offered" flags; [7] frozen-list count
     unsigned* bar;
     int* status;
     uint64_t limit_ns;
@@ -144,13 +147,14 @@ __device__ __forceinline__ void chunk_append(uint32_t* lists, uint32_t* counters
     if ((mask >> lane) & 1u) list[base + __popc(mask & ((1u << lane) - 1u))] = mine;
 }
 
-constexpr int kUnroll = 4;  // edges in flight per warp in the node-segment rounds
+constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0, 1)
+constexpr int kWlGroupFlat = 6;   // worklist edges in flight per warp: one root load per endpoint,
+constexpr int kWlGroupHop = 4;    // or two
 
-/// Root of x in forest j for round r (the identity in round 0; one load when the
-/// forests are flat).
-__device__ __forceinline__ uint32_t root_of(const SweepArgs& a, uint32_t x, unsigned lane, int r, bool flat) {
-    if (r == 0) return x;
-    return flat ? __ldcg(a.parent + static_cast<uint64_t>(x) * kLanes + lane) : find32(a.parent, x, lane);
+/// Root of x in forest j in rounds 0 and 1: the identity in round 0; after round 0's
+/// flatten every node holds its root.
+__device__ __forceinline__ uint32_t root01(const SweepArgs& a, uint32_t x, unsigned lane, int r) {
+    return r == 0 ? x : __ldcg(a.parent + static_cast<uint64_t>(x) * kLanes + lane);
 }
 
 /// Offer `key` to best[root][lane].  The old value is not needed (phase B finds the
@@ -160,9 +164,9 @@ __device__ __forceinline__ void offer_min(const SweepArgs& a, uint32_t root, uns
 }
 
 /// Per-lane two-entry cache of pending offers (root -> smallest key).  Offers to a
-/// root met again soon -- the emitter of consecutive edges, or the few components
-/// of the late rounds, where every edge offers to the same handful of roots -- are
-/// reduced in registers; an atomicMin is issued on eviction and at the flush.
+/// root met again soon -- the few components of the late rounds, where every edge
+/// offers to the same handful of roots -- are reduced in registers; an atomicMin is
+/// issued on eviction and at the flush.
 struct OfferCache {
     uint32_t r0 = kInvalid, r1 = kInvalid;
     unsigned long long k0 = kNoKey, k1 = kNoKey;
@@ -193,18 +197,17 @@ struct OfferCache {
     }
 };
 
-/// Phase A for one edge (i, u, v, w) whose live lanes are `lm` (warp-collective).
-/// With `track`, the edge's new live lanes are stored (always when `fresh`: the
-/// word still holds a previous sweep's value) and a live edge is appended to the next
-/// worklist.  Returns whether this lane offered.
-__device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, uint32_t lm,
-                                           int r, bool flat, bool act, bool track, bool fresh, OfferCache& oc) {
+/// Phase A of rounds 0 and 1 for one bridge edge (i, u, v, w), all lanes
+/// (warp-collective).  In round 1 the edge's live lanes are stored and a live edge
+/// is appended to the next worklist.  Returns whether this lane offered.
+__device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, int r,
+                                             bool act, OfferCache& oc) {
     const unsigned lane = threadIdx.x & 31u;
     bool live = false;
-    if (act && ((lm >> lane) & 1u) && u < a.n && v < a.n) {
+    if (act && u < a.n && v < a.n) {
         const float cu = __ldg(a.core + static_cast<uint64_t>(u) * kLanes + lane);
         const float cv = __ldg(a.core + static_cast<uint64_t>(v) * kLanes + lane);
-        const uint32_t ru = root_of(a, u, lane, r, flat), rv = root_of(a, v, lane, r, flat);
+        const uint32_t ru = root01(a, u, lane, r), rv = root01(a, v, lane, r);
         live = ru != rv;
         if (live) {
             const unsigned long long key = pack_key(max_ref(w, max_ref(cu, cv)), i);
@@ -212,23 +215,193 @@ __device__ __forceinline__ bool edge_lanes(const SweepArgs& a, uint32_t i, uint3
             oc.offer(a, lane, rv, key);
         }
     }
-    if (track) {
+    if (r == 1) {
         const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
-        if (L && (fresh || L != lm) && lane == 0) a.live[i] = L;
         if (L && lane == 0) {
-            const int which = (r + 1) & 1;
-            a.wl[static_cast<uint64_t>(which) * a.E + atomicAdd(a.ctr + which, 1u)] = i;
+            a.live[i] = L;
+            a.wl[static_cast<uint64_t>((r + 1) & 1) * a.E + atomicAdd(a.ctr + ((r + 1) & 1), 1u)] = i;
         }
     }
     return live;
+}
+
+/// Rounds 0 and 1, one chunk of node p's emitted segment (m <= 32 edges b, b+1, ...;
+/// lane t holds edge b+t's other endpoint and base weight).  kSegGroup edges' core
+/// and root loads are issued together; every live edge's key is folded into p's
+/// minimum `seg` (offered once per node by the caller) and offered to the other
+/// endpoint's root through the offer cache.  Round 1 stores the edges' live lanes
+/// and returns the bits of the edges that stay live.
+template <int R>
+__device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, float cp, bool act, uint32_t m,
+                                              uint32_t b, uint32_t my_q, float my_w, unsigned long long& seg,
+                                              OfferCache& oc, uint32_t& live_pairs) {
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t pmask = 0;
+    for (uint32_t t = 0; t < m; t += kSegGroup) {
+        float cq[kSegGroup];
+        uint32_t rq[kSegGroup];
+#pragma unroll
+        for (int x = 0; x < kSegGroup; ++x) {
+            const uint32_t q = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
+            const bool ok = act && t + x < m && q < a.n;
+            cq[x] = ok ? __ldg(a.core + static_cast<uint64_t>(q) * kLanes + lane) : 0.0f;
+            rq[x] = R == 0 ? q : (ok ? __ldcg(a.parent + static_cast<uint64_t>(q) * kLanes + lane) : rp);
+        }
+#pragma unroll
+        for (int x = 0; x < kSegGroup; ++x) {
+            const uint32_t q = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
+            const float w = __shfl_sync(0xFFFFFFFFu, my_w, (t + x) & 31u);
+            const bool lv = act && t + x < m && q < a.n && rp != rq[x];
+            live_pairs += lv ? 1u : 0u;
+            if (lv) {
+                const unsigned long long key = pack_key(max_ref(w, max_ref(cp, cq[x])), b + t + x);
+                seg = key < seg ? key : seg;
+                oc.offer(a, lane, rq[x], key);
+            }
+            // round 1 records the live lanes; the ballot is taken next to its value
+            if (R == 1 && t + x < m) {
+                const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
+                if (L && lane == 0) a.live[b + t + x] = L;
+                if (L) pmask |= 1u << (t + x);
+            }
+        }
+    }
+    return pmask;
+}
+
+/// Rounds 0 and 1: the k-NN edges node by node over the emitted segments (32 edges
+/// of a segment loaded at once); the emitter's offers are reduced in registers and
+/// issued once.  Round 1 also builds round 2's worklist.
+template <int R>
+__device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint32_t nw, bool act, OfferCache& oc,
+                                          uint32_t& live_pairs) {
+    const unsigned lane = threadIdx.x & 31u;
+    bool offered = false;
+    for (uint32_t p = gw; p < a.n; p += nw) {
+        const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
+        if (beg == end) continue;
+        const float cp = act ? __ldg(a.core + static_cast<uint64_t>(p) * kLanes + lane) : 0.0f;
+        const uint32_t rp = act ? root01(a, p, lane, R) : p;
+        unsigned long long seg = kNoKey;
+        for (uint32_t b = beg; b < end; b += 32) {
+            const uint32_t m = min(32u, end - b);
+            uint32_t my_q = 0;
+            float my_w = 0.0f;
+            if (lane < m) {
+                const uint32_t x = __ldg(a.eu + b + lane), y = __ldg(a.ev + b + lane);
+                my_q = x == p ? y : x;
+                my_w = __ldg(a.ew + b + lane);
+            }
+            const uint32_t pmask = seg_chunk<R>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, live_pairs);
+            if (R == 1) chunk_append(a.wl, a.ctr, (R + 1) & 1, a.E, pmask, b + lane);
+        }
+        if (seg != kNoKey) {
+            offer_min(a, rp, lane, seg);
+            offered = true;
+        }
+    }
+    return offered;
+}
+
+/// Rounds >= 2: the worklist of edges live in some MST, 32 entries per warp loaded
+/// at once (index, endpoints, weight, live lanes), a group of them in flight.  With
+/// kFlat every node was flattened after the last round and a root lookup is one
+/// load.  Otherwise it is two: a node holds its root as of the last full flatten (or
+/// a later root that phase B's path halving wrote), which is a node of the frozen
+/// root list or a final root, and the flatten after every phase B points each node
+/// of the frozen list at its current root.  Nothing is written back, so the second
+/// loads of a group are issued together after the first ones.
+template <bool kFlat>
+__device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, bool act,
+                                         OfferCache& oc, uint32_t& live_pairs) {
+    constexpr int G = kFlat ? kWlGroupFlat : kWlGroupHop;
+    const unsigned lane = threadIdx.x & 31u;
+    const int par = r & 1;
+    bool offered = false;
+    const uint32_t cnt = __ldcg(a.ctr + par);
+    const uint32_t* in = a.wl + static_cast<uint64_t>(par) * a.E;
+    for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
+        const uint32_t m = min(32u, cnt - base);
+        uint32_t my_i = 0, my_u = 0, my_v = 0, my_l = 0;
+        float my_w = 0.0f;
+        if (lane < m) {
+            my_i = __ldcg(in + base + lane);
+            my_u = __ldg(a.eu + my_i);
+            my_v = __ldg(a.ev + my_i);
+            my_w = __ldg(a.ew + my_i);
+            my_l = __ldcg(a.live + my_i);
+        }
+        uint32_t pmask = 0;  // entries of this chunk that stay live
+        for (uint32_t t = 0; t < m; t += G) {
+            float cu[G], cv[G];
+            uint32_t ru[G], rv[G];
+            uint32_t okm = 0;
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                const uint32_t src = (t + x) & 31u;
+                const uint32_t u = __shfl_sync(0xFFFFFFFFu, my_u, src);
+                const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, src);
+                const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, src);
+                const bool ok = act && t + x < m && ((l >> lane) & 1u) && u < a.n && v < a.n;
+                okm |= ok ? 1u << x : 0u;
+                cu[x] = ok ? __ldg(a.core + static_cast<uint64_t>(u) * kLanes + lane) : 0.0f;
+                cv[x] = ok ? __ldg(a.core + static_cast<uint64_t>(v) * kLanes + lane) : 0.0f;
+                ru[x] = ok ? __ldcg(a.parent + static_cast<uint64_t>(u) * kLanes + lane) : 0u;
+                rv[x] = ok ? __ldcg(a.parent + static_cast<uint64_t>(v) * kLanes + lane) : 0u;
+            }
+            if (!kFlat) {
+#pragma unroll
+                for (int x = 0; x < G; ++x) {
+                    const uint32_t src = (t + x) & 31u;
+                    const uint32_t u = __shfl_sync(0xFFFFFFFFu, my_u, src);
+                    const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, src);
+                    const bool ok = (okm >> x) & 1u;
+                    if (ok && ru[x] != u) ru[x] = __ldcg(a.parent + static_cast<uint64_t>(ru[x]) * kLanes + lane);
+                    if (ok && rv[x] != v) rv[x] = __ldcg(a.parent + static_cast<uint64_t>(rv[x]) * kLanes + lane);
+                }
+            }
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                const uint32_t src = (t + x) & 31u;
+                const uint32_t i = __shfl_sync(0xFFFFFFFFu, my_i, src);
+                const float w = __shfl_sync(0xFFFFFFFFu, my_w, src);
+                const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, src);
+                const bool lv = ((okm >> x) & 1u) && ru[x] != rv[x];
+                live_pairs += lv ? 1u : 0u;
+                if (lv) {
+                    const unsigned long long key = pack_key(max_ref(w, max_ref(cu[x], cv[x])), i);
+                    oc.offer(a, lane, ru[x], key);
+                    oc.offer(a, lane, rv[x], key);
+                    offered = true;
+                }
+                if (t + x < m) {  // ballot next to the value it reads
+                    const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
+                    if (L && L != l && lane == 0) a.live[i] = L;
+                    if (L) pmask |= 1u << (t + x);
+                }
+            }
+        }
+        chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, my_i);
+    }
+    return offered;
+}
+
+/// Point node c's entry of forest `lane` at its root, if it is not there already
+/// (only ever the final root is written, so concurrent chases stay correct).
+__device__ __forceinline__ void point_at_root(uint32_t* parent, uint32_t c, unsigned lane) {
+    uint32_t* const pc = parent + static_cast<uint64_t>(c) * kLanes + lane;
+    const uint32_t p = __ldcg(pc);
+    if (p == c) return;
+    const uint32_t f = root32(parent, p, lane);
+    if (f != p) *pc = f;
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     const bool act = lane < a.K;
-    const uint32_t allmask = a.K >= 32 ? 0xFFFFFFFFu : ((1u << a.K) - 1u);
     bool flat = true;  // parents are the identity at the start
     int r = 0;
     for (; r < kMaxRounds; ++r) {
@@ -237,144 +410,24 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.ctr[2 + nxt] = 0;  // the root list phase B of this round writes
             a.ctr[5 + nxt] = 0;  // next round's offer flag
-            tr[0] = global_ns();
-            tr[3] = 0;
+            tr[0] = global_ns();  // the other words start zeroed (pre graph)
             tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + par);
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
-            tr[6] = 0;
         }
         OfferCache oc;
         bool offered = false;
         uint32_t live_pairs = 0;
         // ---- phase A
         if (r <= 1) {
-            // k-NN edges, node by node over the emitted segments: 32 edges of a
-            // segment are loaded at once, kUnroll of them are in flight, and the
-            // emitter's offers are reduced in registers and issued once
-            for (uint32_t p = gw; p < a.n; p += nw) {
-                const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
-                if (beg == end) continue;
-                const float cp = act ? __ldg(a.core + static_cast<uint64_t>(p) * kLanes + lane) : 0.0f;
-                const uint32_t rp = act ? root_of(a, p, lane, r, flat) : p;
-                unsigned long long seg = kNoKey;
-                for (uint32_t b = beg; b < end; b += 32) {
-                    const uint32_t m = min(32u, end - b);
-                    uint32_t pmask = 0;  // round 1: edges of this chunk that stay live
-                    uint32_t my_q = 0;
-                    float my_w = 0.0f;
-                    if (lane < m) {
-                        const uint32_t x = __ldg(a.eu + b + lane), y = __ldg(a.ev + b + lane);
-                        my_q = x == p ? y : x;
-                        my_w = __ldg(a.ew + b + lane);
-                    }
-                    for (uint32_t t = 0; t < m; t += kUnroll) {
-                        uint32_t q[kUnroll], rq[kUnroll];
-                        float w[kUnroll], cq[kUnroll];
-                        bool ok[kUnroll];
-#pragma unroll
-                        for (int x = 0; x < kUnroll; ++x) {
-                            q[x] = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
-                            w[x] = __shfl_sync(0xFFFFFFFFu, my_w, (t + x) & 31u);
-                            ok[x] = act && t + x < m && q[x] < a.n;
-                        }
-#pragma unroll
-                        for (int x = 0; x < kUnroll; ++x)
-                            cq[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(q[x]) * kLanes + lane) : 0.0f;
-#pragma unroll
-                        for (int x = 0; x < kUnroll; ++x) rq[x] = ok[x] ? root_of(a, q[x], lane, r, flat) : rp;
-#pragma unroll
-                        for (int x = 0; x < kUnroll; ++x) {
-                            const bool lv = ok[x] && rp != rq[x];
-                            live_pairs += lv ? 1u : 0u;
-                            if (lv) {
-                                const unsigned long long key = pack_key(max_ref(w[x], max_ref(cp, cq[x])), b + t + x);
-                                seg = key < seg ? key : seg;
-                                oc.offer(a, lane, rq[x], key);
-                            }
-                            // round 1 records the live lanes and builds the worklist; the
-                            // ballot is taken here, next to the value it reads
-                            if (r == 1 && t + x < m) {
-                                const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
-                                if (L && lane == 0) a.live[b + t + x] = L;
-                                if (L) pmask |= 1u << (t + x);
-                            }
-                        }
-                    }
-                    if (r == 1) chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, b + lane);
-                }
-                if (seg != kNoKey) {
-                    offer_min(a, rp, lane, seg);
-                    offered = true;
-                }
-            }
+            offered = r == 0 ? seg_round<0>(a, gw, nw, act, oc, live_pairs) : seg_round<1>(a, gw, nw, act, oc, live_pairs);
             // bridges: one warp per edge
             for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
-                const bool o = edge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), allmask, r, flat,
-                                          act, r == 1, true, oc);
+                const bool o = bridge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), r, act, oc);
                 offered = offered || o;
             }
         } else {
-            // the worklist of edges live in some MST: 32 entries per warp loaded at
-            // once (index, endpoints, weight, live lanes), then walked two at a time
-            const uint32_t cnt = __ldcg(a.ctr + par);
-            const uint32_t* in = a.wl + static_cast<uint64_t>(par) * a.E;
-            for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
-                const uint32_t m = min(32u, cnt - base);
-                uint32_t my_i = 0, my_u = 0, my_v = 0, my_l = 0;
-                float my_w = 0.0f;
-                if (lane < m) {
-                    my_i = __ldcg(in + base + lane);
-                    my_u = __ldg(a.eu + my_i);
-                    my_v = __ldg(a.ev + my_i);
-                    my_w = __ldg(a.ew + my_i);
-                    my_l = __ldcg(a.live + my_i);
-                }
-                uint32_t pmask = 0;  // entries of this chunk that stay live
-                for (uint32_t t = 0; t < m; t += kUnroll) {
-                    // kUnroll edges at a time: their core and root loads are issued
-                    // together, then each edge offers and records its live lanes
-                    uint32_t ei[kUnroll], eu[kUnroll], ev[kUnroll], el[kUnroll], ru[kUnroll], rv[kUnroll];
-                    float ew[kUnroll], cu[kUnroll], cv[kUnroll];
-                    bool ok[kUnroll];
-#pragma unroll
-                    for (int x = 0; x < kUnroll; ++x) {
-                        const uint32_t src = (t + x) & 31u;
-                        ei[x] = __shfl_sync(0xFFFFFFFFu, my_i, src);
-                        eu[x] = __shfl_sync(0xFFFFFFFFu, my_u, src);
-                        ev[x] = __shfl_sync(0xFFFFFFFFu, my_v, src);
-                        ew[x] = __shfl_sync(0xFFFFFFFFu, my_w, src);
-                        el[x] = __shfl_sync(0xFFFFFFFFu, my_l, src);
-                        ok[x] = act && t + x < m && ((el[x] >> lane) & 1u) && eu[x] < a.n && ev[x] < a.n;
-                    }
-#pragma unroll
-                    for (int x = 0; x < kUnroll; ++x) {
-                        cu[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(eu[x]) * kLanes + lane) : 0.0f;
-                        cv[x] = ok[x] ? __ldg(a.core + static_cast<uint64_t>(ev[x]) * kLanes + lane) : 0.0f;
-                    }
-#pragma unroll
-                    for (int x = 0; x < kUnroll; ++x) {
-                        ru[x] = ok[x] ? root_of(a, eu[x], lane, r, flat) : 0u;
-                        rv[x] = ok[x] ? root_of(a, ev[x], lane, r, flat) : 0u;
-                    }
-#pragma unroll
-                    for (int x = 0; x < kUnroll; ++x) {
-                        const bool lv = ok[x] && ru[x] != rv[x];
-                        live_pairs += lv ? 1u : 0u;
-                        if (lv) {
-                            const unsigned long long key = pack_key(max_ref(ew[x], max_ref(cu[x], cv[x])), ei[x]);
-                            oc.offer(a, lane, ru[x], key);
-                            oc.offer(a, lane, rv[x], key);
-                            offered = true;
-                        }
-                        if (t + x < m) {  // ballot next to the value it reads
-                            const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
-                            if (L && L != el[x] && lane == 0) a.live[ei[x]] = L;
-                            if (L) pmask |= 1u << (t + x);
-                        }
-                    }
-                }
-                chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, my_i);
-            }
+            offered = flat ? wl_round<true>(a, r, gw, nw, act, oc, live_pairs)
+                           : wl_round<false>(a, r, gw, nw, act, oc, live_pairs);
         }
         oc.flush(a, lane);
         {
@@ -415,15 +468,53 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[par] = 0;  // this round's worklist, consumed
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[2] = global_ns();
-        // ---- flatten the forests when the next round has enough work to profit
-        const uint32_t next = r == 0 ? a.E : __ldcg(a.ctr + nxt);
-        flat = a.flatten_div != 0 && static_cast<uint64_t>(next) * a.flatten_div > a.n;
-        if (flat) {
-            for (uint32_t v = gw; v < a.n; v += nw) {
-                if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
+        // ---- flatten.  Step 1 points at its final root every node of the list whose
+        // roots phase B may have linked: in rounds 0 and 1 the list phase B walked
+        // (every node with an edge, so that is a full flatten), later the frozen root
+        // list (roots as of the last full flatten; it holds every root of this round).
+        // Round 1 freezes round 2's root list.
+        {
+            const uint32_t cnt = r == 0 ? a.n : __ldcg(a.ctr + (r == 1 ? 2 + par : 7));
+            const uint32_t* lst = r == 1 ? a.rlist + static_cast<uint64_t>(par) * a.n : a.fl;
+            for (uint32_t t = gw; t < cnt; t += nw) {
+                if (act) point_at_root(a.parent, r == 0 ? t : __ldcg(lst + t), lane);
             }
+            if (r == 1) {
+                const uint32_t nc = __ldcg(a.ctr + 2 + nxt);
+                const uint32_t* src = a.rlist + static_cast<uint64_t>(nxt) * a.n;
+                for (uint32_t t = gt; t < nc; t += nt) a.fl[t] = __ldcg(src + t);
+                if (gt == 0) a.ctr[7] = nc;
+            }
+        }
+        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        // ---- step 2, from round 2 on: every node, when this round's live (edge, MST)
+        // pairs say the next round's second root loads would cost more than a pass over
+        // the nodes; it freezes the next round's root list.  After step 1 a node's entry
+        // is a frozen-list node or a final root, whose entry is its root: two loads.
+        const uint64_t pairs = __ldcg(tr + 6);
+        const bool full =
+            r >= 2 && a.flatten_div != 0 && pairs > static_cast<uint64_t>(a.n) * kLanes / a.flatten_div;
+        if (full) {
+            for (uint32_t v = gw; v < a.n; v += nw) {
+                if (act) {
+                    uint32_t* const pv = a.parent + static_cast<uint64_t>(v) * kLanes + lane;
+                    const uint32_t p = __ldcg(pv);
+                    if (p != v) {
+                        const uint32_t f = __ldcg(a.parent + static_cast<uint64_t>(p) * kLanes + lane);
+                        if (f != p) *pv = f;
+                    }
+                }
+            }
+            const uint32_t nc = __ldcg(a.ctr + 2 + nxt);
+            const uint32_t* src = a.rlist + static_cast<uint64_t>(nxt) * a.n;
+            for (uint32_t t = gt; t < nc; t += nt) a.fl[t] = __ldcg(src + t);
+            if (gt == 0) a.ctr[7] = nc;
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-            if (blockIdx.x == 0 && threadIdx.x == 0) tr[3] = global_ns();
+        }
+        flat = r <= 1 || full;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            tr[3] = global_ns();
+            tr[7] = flat ? 1u : 0u;
         }
     }
     if (r == kMaxRounds) {
@@ -602,7 +693,7 @@ struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
     bool labels = false;
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
-    DevBuf mpts, parent, best, tree, live, wl, rlist, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins,
+    DevBuf mpts, parent, best, tree, live, wl, rlist, fl, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins,
         trace;
     cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
     std::vector<uint32_t> host_mpts;
@@ -649,6 +740,7 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.live = p.live.as<uint32_t>();
     a.wl = p.wl.as<uint32_t>();
     a.rlist = p.rlist.as<uint32_t>();
+    a.fl = p.fl.as<uint32_t>();
     a.trace = p.trace.as<unsigned long long>();
     a.core = p.core.as<float>();
     a.ctr = p.ctr.as<uint32_t>();
@@ -665,6 +757,7 @@ void enqueue_pre(Graph& g, SweepPlan& p) {
     CSB_CUDA(cudaMemsetAsync(p.status.p, 0, 64, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.bar.p, 0, 64, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.ctr.p, 0, 64, c.stream));
+    CSB_CUDA(cudaMemsetAsync(p.trace.p, 0, kMaxRounds * kTraceWords * 8, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.best.p, 0xFF, n * kLanes * 8, c.stream));
     CSB_CUDA(cudaMemsetAsync(p.tree.p, 0, E * 4, c.stream));
 
@@ -797,6 +890,7 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->live.ensure(E * 4);
         p->wl.ensure(2 * E * 4);
         p->rlist.ensure(2 * n * 4);
+        p->fl.ensure(n * 4);
         p->core.ensure(n * kLanes * 4);
         p->ctr.ensure(64);
         p->trace.ensure(kMaxRounds * kTraceWords * 8);
@@ -890,7 +984,7 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
         }
     }
     if (!B) B = 512;
-    if (F == kFlattenAuto) F = 4;
+    if (F == kFlattenAuto) F = 0;  // the frozen root list alone was fastest at n = 1M
     // passes of at most 32 MSTs, chained plans
     SweepPlan** slot = &g.plan;
     for (uint32_t off = 0; off < K; off += kLanes) {
@@ -1051,7 +1145,7 @@ cs_status cs_sweep_trace(cs_graph* gp, uint64_t* out, uint32_t cap_rounds, uint3
             o[2] = (!last && x[3] > x[2]) ? x[3] - x[2] : 0;           // flatten
             o[3] = x[4];
             o[4] = x[5];
-            o[5] = (!last && x[3] > x[2]) ? 1 : 0;
+            o[5] = last ? 0 : x[7];
             o[6] = x[6];
         }
         if (out_rounds) *out_rounds = rounds;
@@ -1084,9 +1178,9 @@ cs_status cs_autotune_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, uint
         CSB_REQUIRE(mpts != nullptr && K > 0, "cs_autotune_sweep: empty mpts");
         const uint32_t saved_b = g->sweep_block, saved_f = g->sweep_flatten;
         float best_ms = 1e30f;
-        uint32_t best_b = 512, best_f = 4;
+        uint32_t best_b = 512, best_f = 0;
         const uint32_t blocks[] = {256, 512};
-        const uint32_t flats[] = {0, 2, 4, 16};
+        const uint32_t flats[] = {0, 1, 2, 4, 16};
         for (uint32_t B : blocks) {
             for (uint32_t F : flats) {
                 g->sweep_block = B;
