@@ -40,6 +40,22 @@ METRIC = "mpts-sweep MSTs/s + build s, n=1M k=32 vs plain GPU path; p50/p99 quer
 FALLBACK_HBM_GBS = 6650.0
 
 
+def profiled_traffic(workload: str, n: int):
+    """DRAM bytes (read + write) of one k_sweep launch on this workload, from the ncu
+    capture summarised in profiles/ (a line `traffic_per_launch_bytes: B workload W n N`),
+    or None when no capture of this workload and size is committed."""
+    import re
+    d = os.path.join(ROOT, "profiles")
+    for f in sorted(os.listdir(d)) if os.path.isdir(d) else []:
+        if not f.startswith("k_sweep_"):
+            continue
+        for line in open(os.path.join(d, f)):
+            m = re.search(r"traffic_per_launch_bytes:\s*(\d+)\s+workload\s+(\S+)\s+n\s+(\d+)", line)
+            if m and m.group(2) == workload and int(m.group(3)) == n:
+                return int(m.group(1)), f
+    return None
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -474,10 +490,12 @@ def main():
     peak, peak_kind = peaks()
     kb = sweep_kernel_bytes(n, E, K)
     achieved = kb / (kernel_ms / 1000.0) / 1e9
+    prof = profiled_traffic(args.workload, n)
     roofline = {"bound": "hbm", "kernel": "k_sweep (persistent Boruvka, 32 MSTs, lane = MST)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes": kb, "kernel_ms": kernel_ms,
-                "traffic": None,
+                "traffic": prof[0] if prof else None,
+                "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/{prof[1]}" if prof else None,
                 "sweep_graph": {"algorithmic_bytes": sweep_bytes(n, E, K), "ms": ms_per_step,
                                 "achieved_gbs": sweep_bytes(n, E, K) / (ms_per_step / 1000.0) / 1e9}}
 
