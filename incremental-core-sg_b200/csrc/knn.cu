@@ -41,8 +41,6 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSlots = 64;         // overflow table slots per node (two-choice hashed)
 constexpr int kCap = 128;          // append buffer per node
 constexpr int kMaxSample = 32;     // smpN ceiling (cuda/cuda_common.cuh:30)
-constexpr int kMaxNewList = 2 * kMaxSample;
-constexpr int kMaxOldList = 4 * kMaxSample;
 
 inline unsigned blocks_for(uint64_t work, int threads = kThreads) {
     uint64_t b = (work + threads - 1) / threads;
@@ -243,7 +241,13 @@ __global__ void k_sample(uint32_t n, uint32_t k, uint32_t smp, const uint32_t* _
     }
 }
 
-/// Local join (one warp per node; rows staged in shared memory).
+/// Staged row pitch in shared memory: four floats more than the row, so the float4
+/// loads of 8 lanes reading 8 different rows fall into 8 different bank groups (a
+/// pitch of 16 or 32 floats put them into two groups or one).
+__host__ __device__ __forceinline__ uint32_t join_pitch(uint32_t stride) { return stride + 4; }
+
+/// Local join (one warp per node; rows staged in shared memory, `rows` of them at
+/// most: 2 x sample new + 4 x sample old).
 __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts, uint32_t n, uint32_t stride,
                                                    uint32_t smp, const uint32_t* __restrict__ new_s,
                                                    const uint32_t* __restrict__ old_s, const uint32_t* __restrict__ ns,
@@ -253,7 +257,8 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
                                                    const uint32_t* __restrict__ rold_cnt, const float* __restrict__ thr,
                                                    CandStore cand, int warps_per_block,
                                                    unsigned long long* __restrict__ evals,
-                                                   const uint32_t* __restrict__ active, uint32_t n_active) {
+                                                   const uint32_t* __restrict__ active, uint32_t n_active,
+                                                   uint32_t rows) {
     extern __shared__ float smem[];
     const int w = threadIdx.x >> 5;
     if (w >= warps_per_block) return;
@@ -261,11 +266,11 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     if (slot >= (active ? n_active : n)) return;
     const uint32_t p = active ? active[slot] : slot;
     const unsigned lane = threadIdx.x & 31u;
-    constexpr int kRows = kMaxNewList + kMaxOldList;
-    // per-warp shared layout: ids[kRows] | thr[kRows] | rows[kRows][stride]
-    uint32_t* s_id = reinterpret_cast<uint32_t*>(smem) + static_cast<size_t>(w) * (2 * kRows + kRows * stride);
-    float* s_thr = reinterpret_cast<float*>(s_id + kRows);
-    float* s_row = s_thr + kRows;
+    const uint32_t pitch = join_pitch(stride);
+    // per-warp shared layout: ids[rows] | thr[rows] | rows[rows][pitch]
+    uint32_t* s_id = reinterpret_cast<uint32_t*>(smem) + static_cast<size_t>(w) * rows * (2 + pitch);
+    float* s_thr = reinterpret_cast<float*>(s_id + rows);
+    float* s_row = s_thr + rows;
 
     // assemble new = sampled new + reverse new, old = sampled old + reverse old
     const uint32_t sn = ns[p], so = nold[p];
@@ -288,21 +293,24 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     for (uint32_t t = lane; t < nT * q4; t += 32) {
         const uint32_t row = t / q4, c4 = t % q4;
         const float4 v = reinterpret_cast<const float4*>(pts + static_cast<uint64_t>(s_id[row]) * stride)[c4];
-        reinterpret_cast<float4*>(s_row + static_cast<size_t>(row) * stride)[c4] = v;
+        reinterpret_cast<float4*>(s_row + static_cast<size_t>(row) * pitch)[c4] = v;
     }
     __syncwarp();
-    // pairs: a in [0, nN), b in [0, nT), b > a when b < nN
-    const uint32_t total = nN * nT;
+    // pairs: a in [0, nN) with every b > a in [0, nT) -- new x new once, new x old;
+    // row a is read by the whole warp at once (a broadcast), the lanes take the b's
     uint32_t my_evals = 0;
-    for (uint32_t q = lane; q < total; q += 32) {
-        const uint32_t a = q / nT, b = q % nT;
-        if (b < nN && b <= a) continue;
-        const uint32_t u1 = s_id[a], u2 = s_id[b];
-        if (u1 == u2) continue;
-        const float r = l2sqr_ref(s_row + static_cast<size_t>(a) * stride, s_row + static_cast<size_t>(b) * stride, stride);
-        ++my_evals;
-        if (r < s_thr[a]) offer(cand, u1, make_key(r, u2));
-        if (r < s_thr[b]) offer(cand, u2, make_key(r, u1));
+    for (uint32_t a = 0; a < nN; ++a) {
+        const float* ra = s_row + static_cast<size_t>(a) * pitch;
+        const uint32_t u1 = s_id[a];
+        const float ta = s_thr[a];
+        for (uint32_t b = a + 1 + lane; b < nT; b += 32) {
+            const uint32_t u2 = s_id[b];
+            if (u1 == u2) continue;
+            const float r = l2sqr_ref(ra, s_row + static_cast<size_t>(b) * pitch, stride);
+            ++my_evals;
+            if (r < ta) offer(cand, u1, make_key(r, u2));
+            if (r < s_thr[b]) offer(cand, u2, make_key(r, u1));
+        }
     }
     if (evals) {
         for (int o = 16; o > 0; o >>= 1) my_evals += __shfl_xor_sync(0xFFFFFFFFu, my_evals, o);
@@ -754,6 +762,7 @@ struct Descent {
     KnnScratch s;
     uint32_t n, k, smp;
     int wpb = 1;
+    uint32_t join_rows = 0;
     size_t smem = 0;
     unsigned long long* d_updates = nullptr;
     unsigned long long* d_evals = nullptr;
@@ -788,12 +797,26 @@ struct Descent {
         k_threshold<<<blocks_for(n), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(), n, k,
                                                              s.thr.as<float>());
         count_launch(c, 2);
-        // join launch shape: as many warps per block as the staged rows allow
-        constexpr int kRows = kMaxNewList + kMaxOldList;
-        const size_t per_warp = (2 * kRows + static_cast<size_t>(kRows) * g.stride) * 4;
-        wpb = static_cast<int>(std::min<size_t>(kWarps, std::max<size_t>(1, (200u * 1024u) / per_warp)));
+        // join launch shape: the staged rows of one node are at most 2 x sample new
+        // and 4 x sample old; the warps per block that keep the most warps resident
+        join_rows = 6 * smp;
+        const size_t per_warp = static_cast<size_t>(join_rows) * (2 + join_pitch(g.stride)) * 4;
+        int dev = 0, max_smem = 0;
+        CSB_CUDA(cudaGetDevice(&dev));
+        CSB_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CSB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+        int best_resident = 0;
+        for (int w = 1; w <= kWarps; ++w) {
+            if (per_warp * w > static_cast<size_t>(max_smem)) break;
+            int occ = 0;
+            CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_join, w * 32, per_warp * w));
+            if (occ * w > best_resident) {
+                best_resident = occ * w;
+                wpb = w;
+            }
+        }
+        if (best_resident == 0) fail(CS_ERR_UNSUPPORTED, "NN-Descent: a join warp's rows do not fit in shared memory");
         smem = per_warp * wpb;
-        CSB_CUDA(cudaFuncSetAttribute(k_join, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         check_launch(c, "NN-Descent setup");
     }
 
@@ -833,7 +856,8 @@ struct Descent {
                                                       s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
                                                       s.rnew.as<uint32_t>(), s.rold.as<uint32_t>(),
                                                       s.rnew_cnt.as<uint32_t>(), s.rold_cnt.as<uint32_t>(),
-                                                      s.thr.as<float>(), store_of(s), wpb, d_evals, active, m);
+                                                      s.thr.as<float>(), store_of(s), wpb, d_evals, active, m,
+                                                      join_rows);
             count_launch(c, 2);
             launch_merge(c, g, s, d_updates);
             check_launch(c, "NN-Descent round");
