@@ -395,8 +395,9 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     CSB_CUDA(cudaMemsetAsync(status, 0, 4, c.stream));
     const uint64_t nk = static_cast<uint64_t>(n) * k;
     // ---- connectivity
-    s.parent.ensure(n * 4ull);
-    s.lab.ensure(n * 4ull);
+    const uint64_t ns = scratch_nodes(g);
+    s.parent.ensure(ns * 4ull);
+    s.lab.ensure(ns * 4ull);
     const uint32_t nb = blocks_for(n);
     s.bc.ensure(nb * 4ull + 64);
     s.ncomp.ensure(64);
@@ -407,10 +408,10 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     launch_labels(c, s.parent.as<uint32_t>(), n, 1, s.lab.as<uint32_t>(), s.bc.as<uint32_t>(),
                   s.ncomp.as<unsigned long long>());
     // ---- hubness
-    s.rdeg.ensure(n * 4ull);
-    s.score.ensure(n * 8ull);
-    s.ks.ensure(n * 8ull);
-    s.kt.ensure(n * 8ull);
+    s.rdeg.ensure(ns * 4ull);
+    s.score.ensure(ns * 8ull);
+    s.ks.ensure(ns * 8ull);
+    s.kt.ensure(ns * 8ull);
     CSB_CUDA(cudaMemsetAsync(s.rdeg.p, 0, n * 4ull, c.stream));
     k_rdeg<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, s.rdeg.as<int>());
     k_score<<<blocks_for(n), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, k,
@@ -441,8 +442,8 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     // ---- selection: budget lowest under (score, rdeg, id)
     const uint32_t cap = static_cast<uint32_t>(budget + 2ull * ncomp + 8);
     s.hist.ensure(256 * 4);
-    s.chosen.ensure(n + 16ull);
-    s.qtaken.ensure(n + 16ull);
+    s.chosen.ensure(ns + 16ull);
+    s.qtaken.ensure(ns + 16ull);
     s.sel.ensure(cap * 4ull);
     s.selcnt.ensure(64);
     CSB_CUDA(cudaMemsetAsync(s.chosen.p, 0, n, c.stream));

@@ -142,6 +142,16 @@ struct Graph {
 
 constexpr uint32_t kFlattenAuto = 0xFFFFFFFEu;
 
+/// Node count that per-graph scratch is sized for: the allocated capacity, which grows
+/// 1.5x at a time, so scratch is reallocated together with the resident arrays and
+/// not at every insert (a fresh device allocation of hundreds of MB took up to a
+/// second on these GPUs).
+inline uint64_t scratch_nodes(const Graph& g) { return g.cap_n > g.n ? g.cap_n : g.n; }
+/// `count` items proportional to the node count, scaled to scratch_nodes.
+inline uint64_t scratch_scale(const Graph& g, uint64_t count) {
+    return g.n ? count * scratch_nodes(g) / g.n + (count * scratch_nodes(g) % g.n ? 1 : 0) : count;
+}
+
 // ---- module entry points (implemented in the .cu files) ----------------------------
 
 // graph.cu

@@ -166,9 +166,10 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
     Ctx& c = *g.ctx;
     const uint32_t n = static_cast<uint32_t>(g.n);
     const uint32_t words = (g.k + 31) / 32;
-    tmp_mask.ensure(static_cast<size_t>(n) * words * sizeof(uint32_t) + 4);
-    tmp_cnt.ensure((static_cast<size_t>(n) + 1) * sizeof(uint32_t));
-    tmp_off.ensure((static_cast<size_t>(n) + 1) * sizeof(uint32_t));
+    const uint64_t ns = scratch_nodes(g);
+    tmp_mask.ensure(ns * words * sizeof(uint32_t) + 4);
+    tmp_cnt.ensure((ns + 1) * sizeof(uint32_t));
+    tmp_off.ensure((ns + 1) * sizeof(uint32_t));
     float* core = nullptr;
     if (reweight) {
         core_buf.ensure(static_cast<size_t>(n) * sizeof(float) + 4);
@@ -190,9 +191,12 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
     CSB_CUDA(cudaStreamSynchronize(c.stream));
     const uint64_t total = static_cast<uint64_t>(e_knn) + g.nb;
     if (total > 0xFFFFFFFEull) fail(CS_ERR_UNSUPPORTED, "edge count exceeds 32-bit edge indices");
-    u.ensure(total * sizeof(uint32_t) + 4);
-    v.ensure(total * sizeof(uint32_t) + 4);
-    w.ensure(total * sizeof(float) + 4);
+    // the graph's cached edge list is sized for its capacity (it is rebuilt after
+    // every insert)
+    const uint64_t room = &u == &g.eu ? std::max(scratch_scale(g, total), total) : total;
+    u.ensure(room * sizeof(uint32_t) + 4);
+    v.ensure(room * sizeof(uint32_t) + 4);
+    w.ensure(room * sizeof(float) + 4);
     if (n && e_knn) {
         k_edge_emit<<<nb, kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.dists.as<float>(), n, g.k,
                                                    words, tmp_mask.as<uint32_t>(),

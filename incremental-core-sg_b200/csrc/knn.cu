@@ -773,18 +773,19 @@ struct Descent {
         smp = std::min<uint32_t>(std::max<uint32_t>(sample, 1), kMaxSample);
         if (k > 64) fail(CS_ERR_UNSUPPORTED, "NN-Descent: k > 64");
         const uint64_t nk = static_cast<uint64_t>(n) * k;
-        s.thr.ensure(n * 4ull);
-        s.cand.ensure(n * 8ull * kSlots);
-        s.cand_buf.ensure(n * 8ull * kCap);
-        s.cand_cnt.ensure(n * 4ull);
-        s.new_s.ensure(n * 4ull * kMaxSample);
-        s.old_s.ensure(n * 4ull * 3 * kMaxSample);
-        s.ns.ensure(n * 4ull);
-        s.nold.ensure(n * 4ull);
-        s.rnew.ensure(n * 4ull * kMaxSample);
-        s.rold.ensure(n * 4ull * kMaxSample);
-        s.rnew_cnt.ensure(n * 4ull);
-        s.rold_cnt.ensure(n * 4ull);
+        const uint64_t sn = scratch_nodes(g);
+        s.thr.ensure(sn * 4ull);
+        s.cand.ensure(sn * 8ull * kSlots);
+        s.cand_buf.ensure(sn * 8ull * kCap);
+        s.cand_cnt.ensure(sn * 4ull);
+        s.new_s.ensure(sn * 4ull * kMaxSample);
+        s.old_s.ensure(sn * 4ull * 3 * kMaxSample);
+        s.ns.ensure(sn * 4ull);
+        s.nold.ensure(sn * 4ull);
+        s.rnew.ensure(sn * 4ull * kMaxSample);
+        s.rold.ensure(sn * 4ull * kMaxSample);
+        s.rnew_cnt.ensure(sn * 4ull);
+        s.rold_cnt.ensure(sn * 4ull);
         s.counters.ensure(64);
         d_updates = s.counters.as<unsigned long long>();
         d_evals = d_updates + 1;
@@ -956,10 +957,11 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     if (p.reverse_cap) {
         const uint64_t nk = static_cast<uint64_t>(first_new) * k;
         CSB_REQUIRE(nk < 0x7FFFFFFFull, "cs_insert: base graph too large for the reverse index");
-        rev_keys.ensure(nk * 8 + 8);
-        rev_alt.ensure(nk * 8 + 8);
-        rev_deg.ensure(first_new * 4ull + 8);
-        rev_off.ensure(first_new * 4ull + 8);
+        const uint64_t sn = scratch_nodes(g);
+        rev_keys.ensure(sn * k * 8 + 8);
+        rev_alt.ensure(sn * k * 8 + 8);
+        rev_deg.ensure(sn * 4ull + 8);
+        rev_off.ensure(sn * 4ull + 8);
         CSB_CUDA(cudaMemsetAsync(rev_deg.p, 0, first_new * 4ull + 8, c.stream));
         k_rev_keys<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k,
                                                                first_new, rev_keys.as<unsigned long long>(),
@@ -1002,9 +1004,9 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     DevBuf& active = g.insert_scratch[9];
     DevBuf& flag = g.insert_scratch[10];
     DevBuf& off = g.insert_scratch[11];
-    mark.ensure(n + 16ull);
-    firstpos.ensure(n * 4ull);
-    active.ensure(static_cast<uint64_t>(n) * 4 + 4);
+    mark.ensure(scratch_nodes(g) + 16ull);
+    firstpos.ensure(scratch_nodes(g) * 4ull);
+    active.ensure(scratch_nodes(g) * 4 + 4);
     // the active set of a pass: the new points, then two rings, capped.  For the
     // instance (make_anchored_instances, src/incremental_knn.cpp:652-705) ring one is
     // the seeds rank by rank and ring two their neighbours; for the refinement

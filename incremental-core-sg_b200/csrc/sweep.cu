@@ -883,15 +883,17 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         const uint64_t n = std::max<uint32_t>(p->n, 1), E = std::max<uint32_t>(p->E, 1);
         p->ncn = static_cast<uint32_t>((n + 31) / 32);
         p->nce = static_cast<uint32_t>((E + kChunkEdges - 1) / kChunkEdges);
+        // buffers sized for the graph's capacity (grown inserts reuse them)
+        const uint64_t nc = std::max<uint64_t>(scratch_nodes(g), n), Ec = std::max<uint64_t>(scratch_scale(g, E), E);
         p->mpts.ensure(32 * 4);
-        p->parent.ensure(n * kLanes * 4);
-        p->best.ensure(n * kLanes * 8);
-        p->tree.ensure(E * 4);
-        p->live.ensure(E * 4);
-        p->wl.ensure(2 * E * 4);
-        p->rlist.ensure(2 * n * 4);
-        p->fl.ensure(n * 4);
-        p->core.ensure(n * kLanes * 4);
+        p->parent.ensure(nc * kLanes * 4);
+        p->best.ensure(nc * kLanes * 8);
+        p->tree.ensure(Ec * 4);
+        p->live.ensure(Ec * 4);
+        p->wl.ensure(2 * Ec * 4);
+        p->rlist.ensure(2 * nc * 4);
+        p->fl.ensure(nc * 4);
+        p->core.ensure(nc * kLanes * 4);
         p->ctr.ensure(64);
         p->trace.ensure(kMaxRounds * kTraceWords * 8);
         p->bar.ensure(64);
@@ -899,10 +901,10 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->cc.ensure(static_cast<uint64_t>(K) * p->ncn * 4 + 64);
         p->tcnt.ensure(static_cast<uint64_t>(K) * p->nce * 4 + 64);
         if (labels) {
-            p->rootlab.ensure(n * kLanes * 4);
-            p->lab.ensure(static_cast<uint64_t>(K) * n * 4);
+            p->rootlab.ensure(nc * kLanes * 4);
+            p->lab.ensure(static_cast<uint64_t>(K) * nc * 4);
         }
-        p->out.ensure(static_cast<uint64_t>(K) * std::max<uint64_t>(n - 1, 1) * sizeof(cs_edge));
+        p->out.ensure(static_cast<uint64_t>(K) * std::max<uint64_t>(nc - 1, 1) * sizeof(cs_edge));
         p->counts.ensure(64 * 8);
         p->bins.ensure(static_cast<uint64_t>(K) * 256 * 8);
         CSB_CUDA(cudaEventCreate(&p->ev_k0));
