@@ -381,33 +381,12 @@ def main():
         return run_reference(args)
 
     import coresg_b200 as cs
+    from coresg_b200 import replicas
     from coresg_b200.datagen import workload
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = replicas.from_env("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     ctx = cs.Context(local)
     pts, w = workload(args.workload, args.n)
@@ -456,7 +435,7 @@ def main():
     launches = ctx.launches - launches0
     barrier()
     total_ms = max_over_ranks(sum(step_ms))
-    value = world * K * args.steps / (total_ms / 1000.0)
+    value = replicas.replica_throughput(world, K, args.steps, total_ms)
     ms_per_step = total_ms / args.steps
     kernel_ms = float(np.mean(kern_ms))
     log(f"[rank {rank}] sweep {ms_per_step:.3f} ms/step (kernel {kernel_ms:.3f} ms) wall {wall:.3f}s")
@@ -510,6 +489,9 @@ def main():
 
     serving = inserts = highdim = None
     g.close()
+    # the serving, insert and d=128 legs describe one GPU: only a single-rank run has them
+    if world > 1:
+        args.serve_seconds, args.insert_batches, args.highdim = 0, 0, 0
     if args.serve_seconds > 0:
         serving = run_serving(cs, ctx, args)
         log(f"[rank {rank}] serving {serving}")
@@ -538,8 +520,7 @@ def main():
             "clocks": clocks, "wall_s_timed": wall,
         }
         print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
