@@ -452,20 +452,32 @@ def main():
                  "kernel_launches": ctx.launches - ctx_l0,
                  "what": "cs_extract per mpts: edges(mpts) materialised, Boruvka rounds host-driven"}
 
-    # ---- e2e through the C ABI with host buffers
+    # ---- e2e through the C ABI with host buffers: the CORE-SG's k-NN arrays and
+    # bridges in page-locked host memory go up, all K trees and labels come back into
+    # page-locked host arrays, every step
     ids, dists, flags, counts = g.knn()
     bridges = g.missing_edges()
     e2e = None
     if args.e2e_steps > 0:
-        h2d = ids.nbytes + dists.nbytes + flags.nbytes + counts.nbytes + bridges.nbytes
+        def pinned_copy(a):
+            p = cs.Pinned(a.shape, a.dtype)
+            p.array[...] = a
+            return p
+        host_in = [pinned_copy(a) for a in (ids, dists, flags, counts, bridges)]
+        p_ids, p_dists, p_flags, p_counts, p_bridges = (p.array for p in host_in)
+        out_e = cs.Pinned((K, max(n - 1, 1)), cs.EDGE_DTYPE)
+        out_l = cs.Pinned((K, n), np.uint32)
+        h2d = sum(p.array.nbytes for p in host_in)
         secs, d2h = [], 0
         for _ in range(args.e2e_steps):
             t2 = time.perf_counter()
-            g.set_knn(ids, dists, flags, counts)
-            g.set_bridges(bridges)
-            res = g.all_msts(mpts, labels=True)
+            g.set_knn(p_ids, p_dists, p_flags, p_counts)
+            g.set_bridges(p_bridges)
+            res = g.all_msts(mpts, labels=True, out_edges=out_e.array, out_labels=out_l.array)
             secs.append(time.perf_counter() - t2)
             d2h = sum(r.edges.nbytes + r.component.nbytes + 20 for r in res)
+        for p in host_in + [out_e, out_l]:
+            p.free()
         e2e_s = max_over_ranks(sum(secs))
         e2e = {"value": world * K * len(secs) / e2e_s, "unit": "MSTs/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": len(secs)}

@@ -358,13 +358,20 @@ class CoreSG:
                                         C.byref(w)))
         return MstResult(edges[:ne.value], None if lab is None else lab[:n], nc.value, w.value)
 
-    def all_msts(self, mpts_values, labels: bool = True) -> list[MstResult]:
-        """Batched sweep (cs_extract_sweep) -- one persistent graph-captured launch."""
+    def all_msts(self, mpts_values, labels: bool = True, out_edges=None, out_labels=None) -> list[MstResult]:
+        """Batched sweep (cs_extract_sweep) -- one persistent graph-captured launch.
+        out_edges ([K][n-1] EDGE_DTYPE) and out_labels ([K][n] uint32) may be given
+        (page-locked ones, e.g. Pinned arrays, are copied into without staging); the
+        results are views of them."""
         mp = np.ascontiguousarray(mpts_values, np.uint32)
         K, n = len(mp), self.n
         cap = max(n - 1, 1)
-        edges = np.empty((K, cap), EDGE_DTYPE)
-        lab = np.empty((K, max(n, 1)), np.uint32) if labels else None
+        edges = np.empty((K, cap), EDGE_DTYPE) if out_edges is None else out_edges
+        lab = (np.empty((K, max(n, 1)), np.uint32) if out_labels is None else out_labels) if labels else None
+        if edges.dtype != EDGE_DTYPE or edges.shape != (K, cap) or not edges.flags.c_contiguous:
+            raise ValueError("out_edges must be a C-contiguous [K][n-1] edge array")
+        if lab is not None and (lab.dtype != np.uint32 or lab.shape != (K, max(n, 1)) or not lab.flags.c_contiguous):
+            raise ValueError("out_labels must be a C-contiguous [K][n] uint32 array")
         ne = np.empty(K, np.uint64)
         nc = np.empty(K, np.uint32)
         w = np.empty(K, np.float64)

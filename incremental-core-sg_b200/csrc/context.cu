@@ -102,8 +102,25 @@ void Ctx::sync() { CSB_CUDA(cudaStreamSynchronize(stream)); }
 
 /// Host -> device through pinned staging, in 64 MiB chunks so the staging stays
 /// bounded; two staging halves let the memcpy into one overlap the DMA of the other.
+/// Whether a host pointer is page-locked (cudaHostAlloc / cudaHostRegister memory):
+/// such a buffer is copied by the DMA engine directly, without the staging copy.
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
 void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes) {
     if (!bytes) return;
+    if (host_pinned(src)) {
+        CSB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    // pageable: two staging halves, the host copy of one overlapping the DMA of the other
     const size_t chunk = size_t(32) << 20;
     PinnedBuf& st = c.pinned[0];
     st.ensure(2 * std::min(bytes, chunk));
@@ -130,15 +147,36 @@ void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes) {
 
 void copy_d2h(Ctx& c, void* dst, const void* src, size_t bytes) {
     if (!bytes) return;
+    if (host_pinned(dst)) {
+        CSB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    // pageable: two staging halves, the DMA of the next chunk overlapping the host
+    // copy of the current one
     const size_t chunk = size_t(32) << 20;
     PinnedBuf& st = c.pinned[1];
-    st.ensure(std::min(bytes, chunk));
-    for (size_t off = 0; off < bytes; off += st.bytes) {
-        const size_t b = std::min(st.bytes, bytes - off);
-        CSB_CUDA(cudaMemcpyAsync(st.p, static_cast<const char*>(src) + off, b, cudaMemcpyDeviceToHost, c.stream));
-        CSB_CUDA(cudaStreamSynchronize(c.stream));
-        std::memcpy(static_cast<char*>(dst) + off, st.p, b);
+    st.ensure(2 * std::min(bytes, chunk));
+    const size_t half = st.bytes / 2;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    CSB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CSB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    const size_t nchunks = (bytes + half - 1) / half;
+    auto issue = [&](size_t k) {
+        const size_t off = k * half, b = std::min(half, bytes - off);
+        char* stage = static_cast<char*>(st.p) + (k & 1) * half;
+        CSB_CUDA(cudaMemcpyAsync(stage, static_cast<const char*>(src) + off, b, cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaEventRecord(ev[k & 1], c.stream));
+    };
+    issue(0);
+    for (size_t k = 0; k < nchunks; ++k) {
+        if (k + 1 < nchunks) issue(k + 1);  // its half was drained by the host copy of chunk k-1
+        CSB_CUDA(cudaEventSynchronize(ev[k & 1]));
+        const size_t off = k * half, b = std::min(half, bytes - off);
+        std::memcpy(static_cast<char*>(dst) + off, static_cast<char*>(st.p) + (k & 1) * half, b);
     }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
 }
 
 }  // namespace csb
