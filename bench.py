@@ -57,6 +57,33 @@ def profiled_traffic(workload: str, n: int):
     return None
 
 
+def build_recall(g, pts, device: int, queries: int, seed: int) -> dict:
+    """recall@k of the resident k-NN graph against FP32 brute force for a seeded sample
+    of query points (torch on the device, chunks of 500 queries; a measurement only)."""
+    import torch
+
+    n, k = len(pts), g.k_max
+    rng = np.random.default_rng(seed)
+    q = np.sort(rng.choice(n, size=min(queries, n), replace=False))
+    ids, _, _, counts = g.knn()
+    X = torch.from_numpy(np.ascontiguousarray(pts, np.float32)).to(f"cuda:{device}")
+    hits = total = 0
+    for c0 in range(0, len(q), 500):
+        qi = torch.from_numpy(q[c0:c0 + 500]).to(X.device)
+        d = torch.cdist(X[qi], X)  # [b, n]
+        d[torch.arange(len(qi), device=X.device), qi] = float("inf")  # not its own neighbour
+        top = torch.topk(d, k, dim=1, largest=False).indices.cpu().numpy()
+        for r, v in enumerate(q[c0:c0 + 500]):
+            got = ids[v, :counts[v]]
+            hits += len(np.intersect1d(got, top[r], assume_unique=True))
+            total += k
+        del d
+    del X
+    torch.cuda.empty_cache()
+    return {"recall_at_k": hits / total, "k": k, "queries": int(len(q)),
+            "what": "k-NN lists of the device build vs FP32 brute force (torch.cdist), sampled queries"}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -408,6 +435,11 @@ def main():
     t0 = time.perf_counter()
     st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42 + rank)
     rebuild_s = time.perf_counter() - t0
+    bstats = g.build_stats()
+    d_pts = w["dim"]
+    bstats["gflops"] = 3.0 * d_pts * bstats["distance_evals"] / (bstats["device_ms"] / 1000.0) / 1e9
+    bstats["evals_per_node_round"] = bstats["distance_evals"] / (n * max(st.get("rounds", 1), 1))
+    recall = build_recall(g, pts, local, queries=10000, seed=7) if rank == 0 else None
     info = g.info()
     E = info["knn_edges"] + info["bridges"]
     log(f"[rank {rank}] build {build_s:.3f}s (again on the same graph {rebuild_s:.3f}s) {st} |E|={E}")
@@ -523,7 +555,8 @@ def main():
                        "edges": E, "knn_edges": info["knn_edges"], "bridges": info["bridges"],
                        "sweep_flatten_div": flatten, "sweep_block": block,
                        "l2": "inputs larger than L2 (edge list 12 B x |E|), no flush"},
-            "build_s": build_s, "rebuild_s": rebuild_s, "build": st, "first_use_s": first_use_s,
+            "build_s": build_s, "rebuild_s": rebuild_s, "build": st, "build_device": bstats,
+            "build_recall": recall, "first_use_s": first_use_s,
             "plain": plain, "speedup_vs_plain": (value / world) / plain["value"] if plain else None,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "p50_query_ms": serving["p50_query_ms"] if serving else None,

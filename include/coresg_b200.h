@@ -153,6 +153,10 @@ cs_status cs_graph_load(cs_ctx* ctx, const char* path, cs_graph** out_graph);
  * (include/coresg/nndescent.hpp:45-71).  out_updates, out_rounds may be NULL. */
 cs_status cs_knn_build(cs_graph* g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
                        uint64_t* out_updates, uint32_t* out_rounds);
+/* Of the last cs_knn_build: distance evaluations of the local joins (the statistic
+ * NNDescentStats::distance_evals, include/coresg/nndescent.hpp:73-78; 3 x dim FLOP
+ * each) and device milliseconds of the random fill + rounds. */
+cs_status cs_knn_build_stats(cs_graph* g, uint64_t* out_evals, double* out_device_ms);
 
 /* Parameters of cs_insert; cs_insert_defaults fills the reference's defaults
  * (coresg_cli: sample 16, iters 10, refine-iters 5, context-per-new 2.0,

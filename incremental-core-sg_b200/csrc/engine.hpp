@@ -125,6 +125,9 @@ struct Graph {
 
     // Stages of the last cs_insert.
     cs_insert_stats last_insert{};
+    // Distance evaluations and device ms of the last cs_knn_build.
+    uint64_t last_build_evals = 0;
+    double last_build_ms = 0.0;
 
     // Hubness selection of the last cs_select_bridges.
     std::vector<uint32_t> selected;

@@ -890,10 +890,25 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
     if (out_updates) *out_updates = 0;
     if (out_rounds) *out_rounds = 0;
     if (g.n == 0) return;
+    Ctx& c = *g.ctx;
     Descent d(g, sample);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CSB_CUDA(cudaEventCreate(&e0));
+    CSB_CUDA(cudaEventCreate(&e1));
+    CSB_CUDA(cudaEventRecord(e0, c.stream));
     if (random_fill) d.random_fill(seed);
     const uint64_t upd = d.rounds(nullptr, 0, iters, delta, out_rounds);
     d.finish();
+    CSB_CUDA(cudaEventRecord(e1, c.stream));
+    unsigned long long evals = 0;
+    CSB_CUDA(cudaMemcpyAsync(&evals, d.d_evals, 8, cudaMemcpyDeviceToHost, c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    float ms = 0.0f;
+    CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g.last_build_evals = evals;
+    g.last_build_ms = ms;
     if (out_updates) *out_updates = upd;
 }
 
@@ -1181,6 +1196,14 @@ cs_status cs_insert(cs_graph* gp, const float* rows, uint64_t count, uint32_t ro
         g->last_insert = st.detail;
         if (out_active) *out_active = st.active;
         if (out_updates) *out_updates = st.updates;
+    });
+}
+
+cs_status cs_knn_build_stats(cs_graph* gp, uint64_t* out_evals, double* out_device_ms) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        if (out_evals) *out_evals = g->last_build_evals;
+        if (out_device_ms) *out_device_ms = g->last_build_ms;
     });
 }
 
