@@ -229,7 +229,7 @@ __device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uin
 /// lane t holds edge b+t's other endpoint and base weight).  kSegGroup edges' core
 /// and root loads are issued together; every live edge's key is folded into p's
 /// minimum `seg` (offered once per node by the caller) and offered to the other
-/// endpoint's root through the offer cache.  Round 1 stores the edges' live lanes
+/// endpoint's root.  Round 1 stores the edges' live lanes
 /// and returns the bits of the edges that stay live.
 template <int R>
 __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, float cp, bool act, uint32_t m,
@@ -256,7 +256,13 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
             if (lv) {
                 const unsigned long long key = pack_key(max_ref(w, max_ref(cp, cq[x])), b + t + x);
                 seg = key < seg ? key : seg;
-                oc.offer(a, lane, rq[x], key);
+                // round 0: every receiver is its own root and differs edge to edge, so
+                // the cache would only delay the atomic; from round 1 on it merges offers
+                if (R == 0) {
+                    offer_min(a, rq[x], lane, key);
+                } else {
+                    oc.offer(a, lane, rq[x], key);
+                }
             }
             // round 1 records the live lanes; the ballot is taken next to its value
             if (R == 1 && t + x < m) {

@@ -217,7 +217,7 @@ def test_autotune_picks_a_shape(gpu_ctx):
     z = load_golden("coresg_n6000_d16_k32")
     g = resident(gpu_ctx, z)
     F, B = g.autotune(list(range(1, 9)))
-    assert F in (0, 2, 4, 16) and B in (256, 512)
+    assert F in (0, 1, 2, 4, 16) and B in (256, 512)
     res = g.all_msts(list(range(1, 9)))
     assert np.array_equal(edge_keys(res[7].edges), z["mst_keys_8"])
 
