@@ -11,9 +11,9 @@
 //     lane j is MST j.  Per-node state is node-major -- parent[v][32], best[v][32] --
 //     so a node's state for all 32 MSTs is one 128/256-byte line and every per-node
 //     access of the warp is coalesced;
-//   * membership of edge i in the 32 trees is one bit-packed word tree[i]; liveness
-//     likewise (live[i]); a single worklist of edges still live in any MST serves all
-//     of them;
+//   * membership of edge i in the 32 trees is one bit-packed word tree[i]; a single
+//     worklist of edges still live in any MST serves all of them, each entry carrying
+//     the edge (index, endpoints, weight) and its live lanes as one bit word;
 //   * rounds 0 and 1 walk each node's emitted segment (the node-major enumeration of
 //     src/knn_graph.cpp:132-200), so the emitter-side atomicMin of every lane is
 //     aggregated over the segment in registers and issued once;
@@ -77,8 +77,8 @@ struct SweepArgs {
     uint32_t* parent;          // [n][32]
     unsigned long long* best;  // [n][32]
     uint32_t* tree;            // [E] bit j: edge in MST j
-    uint32_t* live;            // [E] bit j: edge live in MST j
-    uint32_t* wl;              // [2][E]
+    uint4* wl;                 // [2][E] worklist entries: edge index, endpoints, base weight bits
+    uint32_t* live;            // [2][E] per worklist entry, bit j: the edge is live in MST j
     uint32_t* rlist;           // [2][n] roots that took an offer in the previous round
     uint32_t* fl;              // [n] frozen root list: roots as of the last full flatten
     const float* core;         // [n][32] core distance of v at mpts[j]
@@ -145,6 +145,25 @@ __device__ __forceinline__ void chunk_append(uint32_t* lists, uint32_t* counters
     if (lane == 0) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
     if ((mask >> lane) & 1u) list[base + __popc(mask & ((1u << lane) - 1u))] = mine;
+}
+
+/// Append the edge entries of a warp's chunk whose bits are set in `mask` (lane t
+/// holds entry `mine` with live lanes `my_live`) to worklist `which`: one atomicAdd
+/// reserves the count, every marked lane writes its own entry, in lane order.
+__device__ __forceinline__ void chunk_append_edges(const SweepArgs& a, int which, uint32_t mask, uint4 mine,
+                                                   uint32_t my_live) {
+    if (!mask) return;
+    uint4* const list = a.wl + static_cast<uint64_t>(which) * a.E;
+    uint32_t* const lives = a.live + static_cast<uint64_t>(which) * a.E;
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.ctr + which, static_cast<uint32_t>(__popc(mask)));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if ((mask >> lane) & 1u) {
+        const uint32_t at = base + __popc(mask & ((1u << lane) - 1u));
+        list[at] = mine;
+        lives[at] = my_live;
+    }
 }
 
 constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0, 1)
@@ -218,8 +237,10 @@ __device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uin
     if (r == 1) {
         const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
         if (L && lane == 0) {
-            a.live[i] = L;
-            a.wl[static_cast<uint64_t>((r + 1) & 1) * a.E + atomicAdd(a.ctr + ((r + 1) & 1), 1u)] = i;
+            const int which = (r + 1) & 1;
+            const uint32_t at = atomicAdd(a.ctr + which, 1u);
+            a.wl[static_cast<uint64_t>(which) * a.E + at] = make_uint4(i, u, v, __float_as_uint(w));
+            a.live[static_cast<uint64_t>(which) * a.E + at] = L;
         }
     }
     return live;
@@ -234,7 +255,7 @@ __device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uin
 template <int R>
 __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, float cp, bool act, uint32_t m,
                                               uint32_t b, uint32_t my_q, float my_w, unsigned long long& seg,
-                                              OfferCache& oc, uint32_t& live_pairs) {
+                                              OfferCache& oc, uint32_t& live_pairs, uint32_t& my_live) {
     const unsigned lane = threadIdx.x & 31u;
     uint32_t pmask = 0;
     for (uint32_t t = 0; t < m; t += kSegGroup) {
@@ -264,10 +285,11 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
                     oc.offer(a, lane, rq[x], key);
                 }
             }
-            // round 1 records the live lanes; the ballot is taken next to its value
+            // round 1 records the live lanes (the lane holding the edge keeps them);
+            // the ballot is taken next to its value
             if (R == 1 && t + x < m) {
                 const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
-                if (L && lane == 0) a.live[b + t + x] = L;
+                if (lane == t + x) my_live = L;
                 if (L) pmask |= 1u << (t + x);
             }
         }
@@ -291,15 +313,18 @@ __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint3
         unsigned long long seg = kNoKey;
         for (uint32_t b = beg; b < end; b += 32) {
             const uint32_t m = min(32u, end - b);
-            uint32_t my_q = 0;
+            uint32_t my_q = 0, my_x = 0, my_y = 0, my_live = 0;
             float my_w = 0.0f;
             if (lane < m) {
-                const uint32_t x = __ldg(a.eu + b + lane), y = __ldg(a.ev + b + lane);
-                my_q = x == p ? y : x;
+                my_x = __ldg(a.eu + b + lane);
+                my_y = __ldg(a.ev + b + lane);
+                my_q = my_x == p ? my_y : my_x;
                 my_w = __ldg(a.ew + b + lane);
             }
-            const uint32_t pmask = seg_chunk<R>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, live_pairs);
-            if (R == 1) chunk_append(a.wl, a.ctr, (R + 1) & 1, a.E, pmask, b + lane);
+            const uint32_t pmask = seg_chunk<R>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, live_pairs, my_live);
+            if (R == 1)
+                chunk_append_edges(a, (R + 1) & 1, pmask, make_uint4(b + lane, my_x, my_y, __float_as_uint(my_w)),
+                                   my_live);
         }
         if (seg != kNoKey) {
             offer_min(a, rp, lane, seg);
@@ -310,7 +335,9 @@ __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint3
 }
 
 /// Rounds >= 2: the worklist of edges live in some MST, 32 entries per warp loaded
-/// at once (index, endpoints, weight, live lanes), a group of them in flight.  With
+/// at once (each entry carries the edge -- index, endpoints, weight -- and its live
+/// lanes, so no gather by edge index precedes the root loads), a group of them in
+/// flight.  With
 /// kFlat every node was flattened after the last round and a root lookup is one
 /// load.  Otherwise it is two: a node holds its root as of the last full flatten (or
 /// a later root that phase B's path halving wrote), which is a node of the frozen
@@ -325,19 +352,20 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
     const int par = r & 1;
     bool offered = false;
     const uint32_t cnt = __ldcg(a.ctr + par);
-    const uint32_t* in = a.wl + static_cast<uint64_t>(par) * a.E;
+    const uint4* in = a.wl + static_cast<uint64_t>(par) * a.E;
+    const uint32_t* in_live = a.live + static_cast<uint64_t>(par) * a.E;
     for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
         const uint32_t m = min(32u, cnt - base);
-        uint32_t my_i = 0, my_u = 0, my_v = 0, my_l = 0;
-        float my_w = 0.0f;
+        uint4 my_e = make_uint4(0u, 0u, 0u, 0u);
+        uint32_t my_l = 0;
         if (lane < m) {
-            my_i = __ldcg(in + base + lane);
-            my_u = __ldg(a.eu + my_i);
-            my_v = __ldg(a.ev + my_i);
-            my_w = __ldg(a.ew + my_i);
-            my_l = __ldcg(a.live + my_i);
+            my_e = __ldcg(in + base + lane);
+            my_l = __ldcg(in_live + base + lane);
         }
+        const uint32_t my_i = my_e.x, my_u = my_e.y, my_v = my_e.z;
+        const float my_w = __uint_as_float(my_e.w);
         uint32_t pmask = 0;  // entries of this chunk that stay live
+        uint32_t my_new = 0;  // this lane's entry's live lanes after the round
         for (uint32_t t = 0; t < m; t += G) {
             float cu[G], cv[G];
             uint32_t ru[G], rv[G];
@@ -371,7 +399,6 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
                 const uint32_t src = (t + x) & 31u;
                 const uint32_t i = __shfl_sync(0xFFFFFFFFu, my_i, src);
                 const float w = __shfl_sync(0xFFFFFFFFu, my_w, src);
-                const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, src);
                 const bool lv = ((okm >> x) & 1u) && ru[x] != rv[x];
                 live_pairs += lv ? 1u : 0u;
                 if (lv) {
@@ -382,12 +409,12 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
                 }
                 if (t + x < m) {  // ballot next to the value it reads
                     const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
-                    if (L && L != l && lane == 0) a.live[i] = L;
+                    if (lane == t + x) my_new = L;
                     if (L) pmask |= 1u << (t + x);
                 }
             }
         }
-        chunk_append(a.wl, a.ctr, (r + 1) & 1, a.E, pmask, my_i);
+        chunk_append_edges(a, (r + 1) & 1, pmask, my_e, my_new);
     }
     return offered;
 }
@@ -744,7 +771,7 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.best = p.best.as<unsigned long long>();
     a.tree = p.tree.as<uint32_t>();
     a.live = p.live.as<uint32_t>();
-    a.wl = p.wl.as<uint32_t>();
+    a.wl = p.wl.as<uint4>();
     a.rlist = p.rlist.as<uint32_t>();
     a.fl = p.fl.as<uint32_t>();
     a.trace = p.trace.as<unsigned long long>();
@@ -895,8 +922,8 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->parent.ensure(nc * kLanes * 4);
         p->best.ensure(nc * kLanes * 8);
         p->tree.ensure(Ec * 4);
-        p->live.ensure(Ec * 4);
-        p->wl.ensure(2 * Ec * 4);
+        p->live.ensure(2 * Ec * 4);
+        p->wl.ensure(2 * Ec * 16);
         p->rlist.ensure(2 * nc * 4);
         p->fl.ensure(nc * 4);
         p->core.ensure(nc * kLanes * 4);
