@@ -5,8 +5,9 @@
 // pass share everything that can be shared:
 //
 //   * the edge list is built once per CORE-SG (graph.cu) and reweighted on the fly,
-//     w'_j = max(w, core_j(u), core_j(v)), with core_j read from the k-NN distance
-//     row of the node (one 128-byte row holds every core distance of a node);
+//     w'_j = max(w, core_j(u), core_j(v)), with core_j read from a [n][32] table of
+//     every node's core distances at the pass's mpts (one 128-byte row per node, built
+//     from the k-NN distance rows in the captured pre graph);
 //   * one warp handles one edge (or one node's emitted segment) for all MSTs at once:
 //     lane j is MST j.  Per-node state is node-major -- parent[v][32], best[v][32] --
 //     so a node's state for all 32 MSTs is one 128/256-byte line and every per-node
@@ -29,10 +30,13 @@
 //
 // Per round r, lane j (MST j):
 //   A  every live edge finds the roots of its endpoints; if they differ it offers the
-//      key (w'_j bits << 32 | i) to best[root][j] of both with atomicMin; the first
-//      offer to a root in a round records the root in the touched list;
-//   B  every touched root takes best[root][j]; the first lane to set bit j of tree[i]
-//      unites the endpoints (roots linked larger-under-smaller) and resets best.
+//      key (w'_j bits << 32 | i) to best[root][j] of both with atomicMin (no result
+//      is read back);
+//   B  every root of the round's root list (every node in round 0; later the roots
+//      that took an offer the round before -- a root without one is final) takes
+//      best[root][j]; the first lane to set bit j of tree[i] unites the endpoints
+//      (roots linked larger-under-smaller) and resets best; the roots that took an
+//      offer form the next round's list.
 // The result is the unique minimum spanning forest of each mpts under (weight bits,
 // edge index), i.e. the reference Boruvka's tree (pack_edge, src/mst.cpp:19-24).
 #include <algorithm>
