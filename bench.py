@@ -240,12 +240,15 @@ def run_inserts(cs, ctx, args):
 
     pts, w = workload(args.insert_workload)
     g = cs.CoreSG(ctx, w["dim"], w["k_max"])
+    rng = np.random.default_rng(w["seed"] + 1)
+    sizes = [int(x) for x in rng.integers(10_000, 200_001, size=args.insert_batches)]
+    # capacity for the base and every batch (Dataset::reserve): the inserts allocate
+    # no device memory
+    g.reserve(w["n"] + sum(sizes))
     t0 = time.perf_counter()
     g.build(pts, sample=16, iters=10, delta=0.001, seed=44)
     build_s = time.perf_counter() - t0
     del pts
-    rng = np.random.default_rng(w["seed"] + 1)
-    sizes = [int(x) for x in rng.integers(10_000, 200_001, size=args.insert_batches)]
     batches = [insert_batch(w, sz, 1000 + i, new_clusters=10 if i % 2 else 0) for i, sz in enumerate(sizes)]
     per, rows, secs = [], 0, 0.0
     for b in batches:
@@ -260,7 +263,8 @@ def run_inserts(cs, ctx, args):
     n_end = g.n
     g.close()
     return {"workload": args.insert_workload, "n_start": w["n"], "n_end": int(n_end), "k_max": w["k_max"],
-            "build_s": build_s, "batches": len(batches), "rows": rows, "seconds": secs,
+            "build_s": build_s, "reserved_rows": w["n"] + sum(sizes), "batches": len(batches), "rows": rows,
+            "seconds": secs,
             "rows_per_s": rows / secs if secs else None, "per_batch": per,
             "what": "cs_insert per batch: seeding search, instance descent, refinement, bridges re-selected"}
 
@@ -308,13 +312,16 @@ def run_serving(cs, ctx, args):
     build_s = time.perf_counter() - t0
     del pts
     stream = request_stream(args.serve_seconds, args.serve_rate, K, seed=w["seed"])
+    batches = {i: insert_batch(w, a.size, a.seed) for i, a in enumerate(stream) if a.kind == CS_REQ_INSERT}
+    n_max = n0 + sum(len(b) for b in batches.values())
+    # capacity for every row the stream will insert (Dataset::reserve), so the window
+    # allocates no device memory; the sweep below then sizes its buffers for it too
+    g.reserve(n_max)
     # epsilon values: quantiles of each mpts tree's merge heights on the built graph
     mp = list(range(1, K + 1))
     g.sweep_device(mp)
     grid = np.linspace(0.0, 1.0, 101)
     qs = {m: np.quantile(g.sweep_fetch(m - 1, labels=False).edges["w"][::16], grid) for m in mp}
-    batches = {i: insert_batch(w, a.size, a.seed) for i, a in enumerate(stream) if a.kind == CS_REQ_INSERT}
-    n_max = n0 + sum(len(b) for b in batches.values())
     pool = [Pinned((3 * n_max,), np.uint32) for _ in range(args.serve_buffers)]
     free = queue.Queue()
     for i in range(len(pool)):

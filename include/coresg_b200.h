@@ -133,6 +133,13 @@ cs_status cs_graph_get_knn(cs_graph* g, uint32_t* ids, float* dists, uint8_t* fl
  * include/coresg/coresg.hpp:155). */
 cs_status cs_graph_set_bridges(cs_graph* g, const cs_edge* edges, uint64_t m);
 cs_status cs_graph_get_bridges(cs_graph* g, cs_edge* out, uint64_t cap, uint64_t* out_count);
+/* Capacity for `rows` nodes (Dataset::reserve, include/coresg/dataset.hpp:50): the
+ * resident arrays and the node-proportional scratch of NN-Descent, inserts and the
+ * bridge selection are allocated for that many nodes now, and the edge list and
+ * sweep buffers are sized for it when next built, so inserts that stay within it
+ * allocate no device memory (a fresh allocation of a few hundred MB took from a few
+ * ms to over a second here).  Never shrinks. */
+cs_status cs_graph_reserve(cs_graph* g, uint64_t rows);
 /* n, k_max, dim, stride, undirected k-NN edge count (KnnGraph::undirected_edge_count,
  * src/knn_graph.cpp:202-217), bridge count.  Any pointer may be NULL. */
 cs_status cs_graph_info(cs_graph* g, uint64_t* n, uint32_t* k_max, uint32_t* dim,

@@ -62,6 +62,7 @@ _SIGS = {
     "cs_graph_load": (_i32, [_p, C.c_char_p, _pp]),
     "cs_knn_build": (_i32, [_p, _u32, _u32, _f64, _u64, _p, _p]),
     "cs_knn_build_stats": (_i32, [_p, _p, _p]),
+    "cs_graph_reserve": (_i32, [_p, _u64]),
     "cs_select_bridges": (_i32, [_p, _p, _p, _p, _p]),
     "cs_insert_defaults": (None, [_p]),
     "cs_insert": (_i32, [_p, _p, _u64, _u32, _p, _p, _p]),
@@ -298,6 +299,10 @@ class CoreSG:
         upd, rounds = C.c_uint64(), C.c_uint32()
         self.ctx.check(lib().cs_knn_build(self.h, sample, iters, delta, seed, C.byref(upd), C.byref(rounds)))
         return dict(updates=upd.value, rounds=rounds.value)
+
+    def reserve(self, rows: int):
+        """Dataset::reserve: capacity (arrays and scratch) for `rows` nodes now."""
+        self.ctx.check(lib().cs_graph_reserve(self.h, int(rows)))
 
     def build_stats(self) -> dict:
         """Distance evaluations and device ms of the last build_knn (cs_knn_build_stats)."""

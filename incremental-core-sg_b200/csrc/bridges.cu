@@ -279,6 +279,18 @@ struct Scratch {
           pintree(g.bridge_scratch[20]), pout(g.bridge_scratch[21]), pcnt(g.bridge_scratch[22]) {}
 };
 
+/// The node-proportional selection scratch for `ns` nodes.
+void size_bridge_scratch(Scratch& s, uint64_t ns) {
+    s.parent.ensure(ns * 4ull);
+    s.lab.ensure(ns * 4ull);
+    s.rdeg.ensure(ns * 4ull);
+    s.score.ensure(ns * 8ull);
+    s.ks.ensure(ns * 8ull);
+    s.kt.ensure(ns * 8ull);
+    s.chosen.ensure(ns + 16ull);
+    s.qtaken.ensure(ns + 16ull);
+}
+
 /// out[i] = (key_a[idx[i]], key_b[idx[i]]): the sort keys of the selected ids.
 __global__ void k_gather_keys(const uint32_t* __restrict__ idx, uint32_t m, const unsigned long long* __restrict__ a,
                               const unsigned long long* __restrict__ b, unsigned long long* __restrict__ out) {
@@ -382,6 +394,11 @@ void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metri
     k_mrd<<<blocks_for(cells), kThreads, 0, c.stream>>>(d_pts, m, stride, metric, d_core, r0, r1 - r0, d_out);
     count_launch(c);
     check_launch(c, "mrd rows");
+}
+
+void bridges_reserve(Graph& g) {
+    Scratch s(g);
+    size_bridge_scratch(s, scratch_nodes(g));
 }
 
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,

@@ -195,6 +195,8 @@ void launch_labels(Ctx& c, uint32_t* parent_all, uint32_t n, uint32_t K, uint32_
 void launch_scan_tiles(Ctx& c, uint32_t* tiles, uint32_t nt, uint32_t K, unsigned long long* totals);
 
 // knn.cu
+/// Allocate the NN-Descent and insert scratch for scratch_nodes(g) nodes now.
+void knn_reserve(Graph& g);
 void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64_t seed,
                  bool random_fill, uint64_t* out_updates, uint32_t* out_rounds);
 struct InsertStats {
@@ -207,6 +209,8 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
                 InsertStats* st);
 
 // bridges.cu
+/// Allocate the selection scratch for scratch_nodes(g) nodes now.
+void bridges_reserve(Graph& g);
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
                     uint32_t* out_components);
 void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metric,

@@ -441,6 +441,16 @@ cs_status cs_graph_info(cs_graph* gp, uint64_t* n, uint32_t* k_max, uint32_t* di
     });
 }
 
+cs_status cs_graph_reserve(cs_graph* gp, uint64_t rows) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(rows < 0xFFFFFFFFull, "cs_graph_reserve: too many rows for 32-bit ids");
+        if (rows > g->cap_n) g->ensure_capacity(rows, true);
+        knn_reserve(*g);
+        bridges_reserve(*g);
+    });
+}
+
 cs_status cs_core_distances(cs_graph* gp, uint32_t mpts, float* host_out) {
     Graph* g = reinterpret_cast<Graph*>(gp);
     return guarded(g ? g->ctx : nullptr, [&] {

@@ -726,6 +726,35 @@ struct KnnScratch {
           counters(g.knn_scratch[12]) {}
 };
 
+/// The node-proportional NN-Descent scratch for `sn` nodes.
+void size_descent_scratch(KnnScratch& s, uint64_t sn) {
+    s.thr.ensure(sn * 4ull);
+    s.cand.ensure(sn * 8ull * kSlots);
+    s.cand_buf.ensure(sn * 8ull * kCap);
+    s.cand_cnt.ensure(sn * 4ull);
+    s.new_s.ensure(sn * 4ull * kMaxSample);
+    s.old_s.ensure(sn * 4ull * 3 * kMaxSample);
+    s.ns.ensure(sn * 4ull);
+    s.nold.ensure(sn * 4ull);
+    s.rnew.ensure(sn * 4ull * kMaxSample);
+    s.rold.ensure(sn * 4ull * kMaxSample);
+    s.rnew_cnt.ensure(sn * 4ull);
+    s.rold_cnt.ensure(sn * 4ull);
+    s.counters.ensure(64);
+}
+
+/// The node-proportional insert scratch (reverse index, active-set marks) for `sn`
+/// nodes.
+void size_insert_scratch(Graph& g, uint64_t sn) {
+    g.insert_scratch[2].ensure(sn * g.k * 8 + 8);  // reverse keys
+    g.insert_scratch[3].ensure(sn * g.k * 8 + 8);  // their sort buffer
+    g.insert_scratch[4].ensure(sn * 4ull + 8);     // reverse degrees
+    g.insert_scratch[5].ensure(sn * 4ull + 8);     // reverse offsets
+    g.insert_scratch[7].ensure(sn + 16ull);        // active-set marks
+    g.insert_scratch[8].ensure(sn * 4ull);         // first positions
+    g.insert_scratch[9].ensure(sn * 4 + 4);        // active set
+}
+
 CandStore store_of(KnnScratch& s) {
     CandStore cs;
     cs.buf = s.cand_buf.as<unsigned long long>();
@@ -773,20 +802,7 @@ struct Descent {
         smp = std::min<uint32_t>(std::max<uint32_t>(sample, 1), kMaxSample);
         if (k > 64) fail(CS_ERR_UNSUPPORTED, "NN-Descent: k > 64");
         const uint64_t nk = static_cast<uint64_t>(n) * k;
-        const uint64_t sn = scratch_nodes(g);
-        s.thr.ensure(sn * 4ull);
-        s.cand.ensure(sn * 8ull * kSlots);
-        s.cand_buf.ensure(sn * 8ull * kCap);
-        s.cand_cnt.ensure(sn * 4ull);
-        s.new_s.ensure(sn * 4ull * kMaxSample);
-        s.old_s.ensure(sn * 4ull * 3 * kMaxSample);
-        s.ns.ensure(sn * 4ull);
-        s.nold.ensure(sn * 4ull);
-        s.rnew.ensure(sn * 4ull * kMaxSample);
-        s.rold.ensure(sn * 4ull * kMaxSample);
-        s.rnew_cnt.ensure(sn * 4ull);
-        s.rold_cnt.ensure(sn * 4ull);
-        s.counters.ensure(64);
+        size_descent_scratch(s, scratch_nodes(g));
         d_updates = s.counters.as<unsigned long long>();
         d_evals = d_updates + 1;
         CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
@@ -939,6 +955,12 @@ uint32_t expand_ring(Ctx& c, Graph& g, const uint32_t* src, uint32_t ns, uint8_t
     return std::min(total, limit);
 }
 
+void knn_reserve(Graph& g) {
+    KnnScratch s(g);
+    size_descent_scratch(s, scratch_nodes(g));
+    size_insert_scratch(g, scratch_nodes(g));
+}
+
 void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride, const cs_insert_params& p,
                 InsertStats* st) {
     Ctx& c = *g.ctx;
@@ -972,11 +994,7 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     if (p.reverse_cap) {
         const uint64_t nk = static_cast<uint64_t>(first_new) * k;
         CSB_REQUIRE(nk < 0x7FFFFFFFull, "cs_insert: base graph too large for the reverse index");
-        const uint64_t sn = scratch_nodes(g);
-        rev_keys.ensure(sn * k * 8 + 8);
-        rev_alt.ensure(sn * k * 8 + 8);
-        rev_deg.ensure(sn * 4ull + 8);
-        rev_off.ensure(sn * 4ull + 8);
+        size_insert_scratch(g, scratch_nodes(g));
         CSB_CUDA(cudaMemsetAsync(rev_deg.p, 0, first_new * 4ull + 8, c.stream));
         k_rev_keys<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), k,
                                                                first_new, rev_keys.as<unsigned long long>(),
@@ -1019,9 +1037,7 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
     DevBuf& active = g.insert_scratch[9];
     DevBuf& flag = g.insert_scratch[10];
     DevBuf& off = g.insert_scratch[11];
-    mark.ensure(scratch_nodes(g) + 16ull);
-    firstpos.ensure(scratch_nodes(g) * 4ull);
-    active.ensure(scratch_nodes(g) * 4 + 4);
+    size_insert_scratch(g, scratch_nodes(g));
     // the active set of a pass: the new points, then two rings, capped.  For the
     // instance (make_anchored_instances, src/incremental_knn.cpp:652-705) ring one is
     // the seeds rank by rank and ring two their neighbours; for the refinement

@@ -106,6 +106,30 @@ def test_sweep_into_pinned_outputs(gpu_ctx):
             p.free()
 
 
+def test_reserve_keeps_the_graph(gpu_ctx):
+    """cs_graph_reserve grows the resident arrays in place (contents kept) and sizes the
+    scratch for the capacity: trees before and after are identical, also when the
+    capacity was reserved before any data arrived."""
+    z = load_golden("coresg_n6000_d16_k32")
+    n = len(z["counts"])
+    g = resident(gpu_ctx, z)
+    mp = [2, 8, 32]
+    before = g.all_msts(mp)
+    g.reserve(3 * n)
+    ids, dists, _, counts = g.knn()
+    assert np.array_equal(ids, z["ids"]) and np.array_equal(dists, z["dists"]) and np.array_equal(counts, z["counts"])
+    after = g.all_msts(mp)
+    g2 = cs.CoreSG(gpu_ctx, int(z["dim"]), int(z["k"]))
+    g2.reserve(2 * n)
+    g2.set_knn(z["ids"], z["dists"], z["flags"], z["counts"])
+    g2.set_bridges(z["bridges"])
+    fresh = g2.all_msts(mp)
+    for a, b, c in zip(before, after, fresh):
+        assert a.edges.tobytes() == b.edges.tobytes() == c.edges.tobytes()
+        assert np.array_equal(a.component, b.component) and np.array_equal(a.component, c.component)
+        assert a.weight == b.weight == c.weight
+
+
 def test_full_sweep_1_to_kmax_repeats_and_zero(gpu_ctx, oracle):
     """All mpts 1..k_max, a repeated value and mpts 0 (== 1): 34 MSTs, so two passes."""
     z = load_golden("coresg_n6000_d16_k32")
