@@ -150,6 +150,15 @@ cs_status cs_graph_info(cs_graph* g, uint64_t* n, uint32_t* k_max, uint32_t* dim
  * Connectivity and hubness are derived state and are not stored (as in the
  * reference); cs_select_bridges recomputes them. */
 cs_status cs_graph_save(cs_graph* g, const char* path);
+/* The extraction's text outputs, byte for byte as coresg::write_edges_tsv /
+ * write_labels_tsv (src/io.cpp:131-145, apps/coresg_cli.cpp:563-570): "u\tv\tweight"
+ * with the weight in scientific notation, 9 digits; "id\tlabel". */
+cs_status cs_write_edges_tsv(const char* path, const cs_edge* edges, uint64_t m);
+cs_status cs_write_labels_tsv(const char* path, const uint32_t* labels, uint64_t n);
+/* Result `index` of the last sweep (its tree, and its labels when the sweep computed
+ * them) straight from the device to those files; either path may be NULL. */
+cs_status cs_sweep_write_tsv(cs_graph* g, uint32_t index, const char* edges_path,
+                             const char* labels_path);
 cs_status cs_graph_load(cs_ctx* ctx, const char* path, cs_graph** out_graph);
 
 /* ---- build: NN-Descent on the resident points + bridges --------------------- */

@@ -63,6 +63,9 @@ _SIGS = {
     "cs_knn_build": (_i32, [_p, _u32, _u32, _f64, _u64, _p, _p]),
     "cs_knn_build_stats": (_i32, [_p, _p, _p]),
     "cs_graph_reserve": (_i32, [_p, _u64]),
+    "cs_write_edges_tsv": (_i32, [C.c_char_p, _p, _u64]),
+    "cs_write_labels_tsv": (_i32, [C.c_char_p, _p, _u64]),
+    "cs_sweep_write_tsv": (_i32, [_p, _u32, C.c_char_p, C.c_char_p]),
     "cs_select_bridges": (_i32, [_p, _p, _p, _p, _p]),
     "cs_insert_defaults": (None, [_p]),
     "cs_insert": (_i32, [_p, _p, _u64, _u32, _p, _p, _p]),
@@ -95,6 +98,20 @@ def header_symbols(path: str = HEADER_PATH) -> list[str]:
     """Every function name declared in include/coresg_b200.h."""
     text = open(path).read()
     return sorted(set(re.findall(r"\b(cs_[a-z0-9_]+)\s*\(", text)))
+
+
+def write_edges_tsv(path, edges) -> None:
+    """coresg::write_edges_tsv (cs_write_edges_tsv) of a host edge array."""
+    e = np.ascontiguousarray(edges, EDGE_DTYPE)
+    if lib().cs_write_edges_tsv(str(path).encode(), _ptr(e), len(e)) != CS_OK:
+        raise CsError(CS_ERR_INVALID, lib().cs_last_error(None).decode())
+
+
+def write_labels_tsv(path, labels) -> None:
+    """coresg::write_labels_tsv (cs_write_labels_tsv) of a host label array."""
+    lab = np.ascontiguousarray(labels, np.uint32)
+    if lib().cs_write_labels_tsv(str(path).encode(), _ptr(lab), len(lab)) != CS_OK:
+        raise CsError(CS_ERR_INVALID, lib().cs_last_error(None).decode())
 
 
 def lib() -> C.CDLL:
@@ -299,6 +316,11 @@ class CoreSG:
         upd, rounds = C.c_uint64(), C.c_uint32()
         self.ctx.check(lib().cs_knn_build(self.h, sample, iters, delta, seed, C.byref(upd), C.byref(rounds)))
         return dict(updates=upd.value, rounds=rounds.value)
+
+    def write_sweep_tsv(self, index: int, edges_path=None, labels_path=None):
+        """Result `index` of the last sweep straight to TSV files (cs_sweep_write_tsv)."""
+        enc = lambda p: None if p is None else str(p).encode()
+        self.ctx.check(lib().cs_sweep_write_tsv(self.h, index, enc(edges_path), enc(labels_path)))
 
     def reserve(self, rows: int):
         """Dataset::reserve: capacity (arrays and scratch) for `rows` nodes now."""

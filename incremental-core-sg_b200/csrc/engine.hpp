@@ -252,6 +252,25 @@ cs_status guarded(Ctx* c, F&& f) {
     }
 }
 
+/// Run f for an entry point that needs no device (host formatting): exceptions
+/// become the status and the thread's last error.
+template <typename F>
+cs_status host_guarded(F&& f) {
+    try {
+        f();
+        return CS_OK;
+    } catch (const Error& e) {
+        set_thread_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_thread_error("host allocation failed");
+        return CS_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_thread_error(e.what());
+        return CS_ERR_INVALID;
+    }
+}
+
 void ctx_free(Ctx* c);
 
 // launch bookkeeping

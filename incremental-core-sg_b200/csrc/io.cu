@@ -52,6 +52,32 @@ std::vector<T> get_vec(FILE* f, uint64_t expect) {
 }
 
 }  // namespace
+/// write_edges_tsv (src/io.cpp:131-138): a "u\tv\tweight" header, then one line per
+/// edge with the weight in std::scientific at precision 9 (the float widened to
+/// double, as the stream formats it: printf's %.9e).
+void write_edges_tsv_file(const char* path, const cs_edge* edges, uint64_t m) {
+    File file(std::fopen(path, "wb"));
+    if (!file.f) fail(CS_ERR_INVALID, std::string("cannot write ") + path);
+    std::vector<char> buf(size_t(1) << 20);
+    std::setvbuf(file.f, buf.data(), _IOFBF, buf.size());
+    std::fputs("u\tv\tweight\n", file.f);
+    for (uint64_t i = 0; i < m; ++i)
+        std::fprintf(file.f, "%u\t%u\t%.9e\n", edges[i].u, edges[i].v, static_cast<double>(edges[i].w));
+    if (std::fflush(file.f) != 0) fail(CS_ERR_INVALID, std::string("cannot write ") + path);
+}
+
+/// write_labels_tsv (src/io.cpp:140-145): an "id\tlabel" header, then "i\tlabel[i]".
+void write_labels_tsv_file(const char* path, const uint32_t* labels, uint64_t n) {
+    File file(std::fopen(path, "wb"));
+    if (!file.f) fail(CS_ERR_INVALID, std::string("cannot write ") + path);
+    std::vector<char> buf(size_t(1) << 20);
+    std::setvbuf(file.f, buf.data(), _IOFBF, buf.size());
+    std::fputs("id\tlabel\n", file.f);
+    for (uint64_t i = 0; i < n; ++i)
+        std::fprintf(file.f, "%llu\t%u\n", static_cast<unsigned long long>(i), labels[i]);
+    if (std::fflush(file.f) != 0) fail(CS_ERR_INVALID, std::string("cannot write ") + path);
+}
+
 }  // namespace csb
 
 using namespace csb;
@@ -155,6 +181,34 @@ cs_status cs_graph_load(cs_ctx* ctx, const char* path, cs_graph** out) {
         }
         reinterpret_cast<Graph*>(gh)->n_repair = repair;
         *out = gh;
+    });
+}
+
+cs_status cs_write_edges_tsv(const char* path, const cs_edge* edges, uint64_t m) {
+    return host_guarded([&] {
+        CSB_REQUIRE(path != nullptr && (edges != nullptr || m == 0), "cs_write_edges_tsv: null argument");
+        write_edges_tsv_file(path, edges, m);
+    });
+}
+
+cs_status cs_write_labels_tsv(const char* path, const uint32_t* labels, uint64_t n) {
+    return host_guarded([&] {
+        CSB_REQUIRE(path != nullptr && (labels != nullptr || n == 0), "cs_write_labels_tsv: null argument");
+        write_labels_tsv_file(path, labels, n);
+    });
+}
+
+cs_status cs_sweep_write_tsv(cs_graph* gp, uint32_t index, const char* edges_path, const char* labels_path) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        MstHost r;
+        sweep_fetch(*g, index, nullptr, nullptr, &r);  // sizes: the sweep's node count is edges + components
+        const uint64_t n = r.nedges + r.ncomp;
+        std::vector<cs_edge> edges(edges_path ? r.nedges : 0);
+        std::vector<uint32_t> labels(labels_path ? n : 0);
+        sweep_fetch(*g, index, edges_path ? edges.data() : nullptr, labels_path ? labels.data() : nullptr, &r);
+        if (edges_path) write_edges_tsv_file(edges_path, edges.data(), r.nedges);
+        if (labels_path) write_labels_tsv_file(labels_path, labels.data(), n);
     });
 }
 

@@ -222,9 +222,23 @@ class Reference:
         _sig(lib, "ref_sampled_recall", _f64, _p, _u64, _u32, _p, _p, _p, _u32, _u64, _u64, _u32)
         _sig(lib, "ref_nndescent", C.c_int, _p, _u64, _u32, _u32, _u32, _u32, _f64, _u64, _u32,
              _p, _p, _p, _p, _p)
+        _sig(lib, "ref_write_edges_tsv", C.c_int, C.c_char_p, _p, _u64)
+        _sig(lib, "ref_write_labels_tsv", C.c_int, C.c_char_p, _p, _u64)
 
     def err(self) -> str:
         return self.lib.ref_last_error().decode()
+
+    def write_edges_tsv(self, path, edges):
+        """coresg::write_edges_tsv (src/io.cpp:131-138)."""
+        e = np.ascontiguousarray(edges, EDGE_DTYPE)
+        if self.lib.ref_write_edges_tsv(str(path).encode(), _ptr(e), len(e)):
+            raise RuntimeError(self.err())
+
+    def write_labels_tsv(self, path, labels):
+        """coresg::write_labels_tsv (src/io.cpp:140-145)."""
+        lab = np.ascontiguousarray(labels, np.uint32)
+        if self.lib.ref_write_labels_tsv(str(path).encode(), _ptr(lab), len(lab)):
+            raise RuntimeError(self.err())
 
     def metric_distance(self, a, b):
         a = np.ascontiguousarray(a, np.float32)

@@ -21,6 +21,7 @@
 
 #include "coresg/coresg.hpp"
 #include "coresg/eval.hpp"
+#include "coresg/io.hpp"
 #include "coresg/mst.hpp"
 #include "coresg/nndescent.hpp"
 #include "coresg/thread_pool.hpp"
@@ -162,6 +163,28 @@ void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
 }
 
 void ref_free(void* hp) { delete static_cast<Handle*>(hp); }
+
+// coresg::write_edges_tsv / write_labels_tsv (src/io.cpp:131-145) on caller arrays
+int ref_write_edges_tsv(const char* path, const void* edges, std::uint64_t m) {
+    try {
+        const auto* e = static_cast<const coresg::Edge*>(edges);
+        coresg::write_edges_tsv(path, std::vector<coresg::Edge>(e, e + m));
+        return 0;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return 1;
+    }
+}
+
+int ref_write_labels_tsv(const char* path, const std::uint32_t* labels, std::uint64_t n) {
+    try {
+        coresg::write_labels_tsv(path, std::vector<coresg::idx_t>(labels, labels + n));
+        return 0;
+    } catch (const std::exception& ex) {
+        g_err = ex.what();
+        return 1;
+    }
+}
 
 int ref_save(void* hp, const char* path) {
     try {

@@ -51,3 +51,23 @@ def test_files_interoperate_with_the_reference(gpu_ctx, tmp_path):
     back = ref.lib.ref_load(p2.encode(), 4)
     assert back
     ref.lib.ref_free(back)
+
+
+def test_sweep_results_straight_to_tsv(gpu_ctx, tmp_path):
+    """cs_sweep_write_tsv writes a sweep's tree and labels from the device in the
+    reference's TSV formats: the same bytes as the host writers (pinned to the
+    reference's own writers by test_tsv.py) on the fetched results."""
+    z = load_golden("coresg_n3000_d24_k16")
+    g = cs.CoreSG(gpu_ctx, int(z["dim"]), int(z["k"]))
+    g.set_knn(z["ids"], z["dists"], z["flags"], z["counts"])
+    g.set_bridges(z["bridges"])
+    mp = [2, 8, 16]
+    res = g.all_msts(mp)
+    for j, r in enumerate(res):
+        g.write_sweep_tsv(j, tmp_path / f"e{j}.tsv", tmp_path / f"l{j}.tsv")
+        cs.write_edges_tsv(tmp_path / f"he{j}.tsv", r.edges)
+        cs.write_labels_tsv(tmp_path / f"hl{j}.tsv", r.component)
+        assert (tmp_path / f"e{j}.tsv").read_bytes() == (tmp_path / f"he{j}.tsv").read_bytes()
+        assert (tmp_path / f"l{j}.tsv").read_bytes() == (tmp_path / f"hl{j}.tsv").read_bytes()
+    g.write_sweep_tsv(0, tmp_path / "only_edges.tsv", None)
+    assert (tmp_path / "only_edges.tsv").read_bytes() == (tmp_path / "he0.tsv").read_bytes()
