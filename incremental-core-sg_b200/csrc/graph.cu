@@ -217,6 +217,16 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
 void graph_build_edges(Graph& g) {
     if (g.edges_valid) return;
     Ctx& c = *g.ctx;
+    // every endpoint of the edge list is a node of the graph: the k-NN edges by
+    // construction (k_edge_mask), the bridges checked here (they may predate a
+    // cs_graph_set_points that shrank the graph); the sweep relies on it
+    if (g.nb) {
+        std::vector<cs_edge> br(g.nb);
+        copy_d2h(c, br.data(), g.bridges.p, g.nb * sizeof(cs_edge));
+        for (const cs_edge& e : br) {
+            if (e.u >= g.n || e.v >= g.n) fail(CS_ERR_STATE, "bridge endpoint out of range for the current graph");
+        }
+    }
     DevBuf core_unused;
     g.e_total = graph_materialize_edges(g, 0, false, g.eu, g.ev, g.ew, core_unused, c.scratch[0],
                                         c.scratch[1], g.node_off);

@@ -171,7 +171,7 @@ __device__ __forceinline__ void chunk_append_edges(const SweepArgs& a, int which
 }
 
 constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0, 1)
-constexpr int kWlGroupFlat = 6;   // worklist edges in flight per warp: one root load per endpoint,
+constexpr int kWlGroupFlat = 4;   // worklist edges in flight per warp: one root load per endpoint,
 constexpr int kWlGroupHop = 4;    // or two
 
 /// Root of x in forest j in rounds 0 and 1: the identity in round 0; after round 0's
@@ -268,7 +268,7 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
 #pragma unroll
         for (int x = 0; x < kSegGroup; ++x) {
             const uint32_t q = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
-            const bool ok = act && t + x < m && q < a.n;
+            const bool ok = act && t + x < m;  // endpoints are nodes (graph_build_edges)
             cq[x] = ok ? __ldg(a.core + static_cast<uint64_t>(q) * kLanes + lane) : 0.0f;
             rq[x] = R == 0 ? q : (ok ? __ldcg(a.parent + static_cast<uint64_t>(q) * kLanes + lane) : rp);
         }
@@ -276,7 +276,7 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
         for (int x = 0; x < kSegGroup; ++x) {
             const uint32_t q = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
             const float w = __shfl_sync(0xFFFFFFFFu, my_w, (t + x) & 31u);
-            const bool lv = act && t + x < m && q < a.n && rp != rq[x];
+            const bool lv = act && t + x < m && rp != rq[x];
             live_pairs += lv ? 1u : 0u;
             if (lv) {
                 const unsigned long long key = pack_key(max_ref(w, max_ref(cp, cq[x])), b + t + x);
@@ -380,7 +380,7 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
                 const uint32_t u = __shfl_sync(0xFFFFFFFFu, my_u, src);
                 const uint32_t v = __shfl_sync(0xFFFFFFFFu, my_v, src);
                 const uint32_t l = __shfl_sync(0xFFFFFFFFu, my_l, src);
-                const bool ok = act && t + x < m && ((l >> lane) & 1u) && u < a.n && v < a.n;
+                const bool ok = act && t + x < m && ((l >> lane) & 1u);
                 okm |= ok ? 1u << x : 0u;
                 cu[x] = ok ? __ldg(a.core + static_cast<uint64_t>(u) * kLanes + lane) : 0.0f;
                 cv[x] = ok ? __ldg(a.core + static_cast<uint64_t>(v) * kLanes + lane) : 0.0f;
