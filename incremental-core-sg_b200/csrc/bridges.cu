@@ -53,7 +53,7 @@ __global__ void k_conn_unite(const uint32_t* __restrict__ ids, const uint32_t* _
     const uint32_t p = static_cast<uint32_t>(t / k), j = static_cast<uint32_t>(t % k);
     if (j >= counts[p]) return;
     const uint32_t q = ids[t];
-    if (q < n && q != p) uf_unite(parent, p, q, status);
+    if (q < n && q != p) uf_unite(parent, p, q, n, status);
 }
 
 __global__ void k_rdeg(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,

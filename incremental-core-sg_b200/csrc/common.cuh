@@ -116,8 +116,11 @@ __device__ __forceinline__ float core_of(const float* dists, const uint32_t* cou
 // src/connectivity.cpp:20-61).  Path halving writes only non-root entries, unions
 // write only roots (by CAS), so concurrent finds and unions are safe.
 
-__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
-    for (;;) {
+/// A set of n nodes has no chain longer than n: a chase that takes more steps (a
+/// cycle, which the linking rule rules out) stops and sets kStatusUnionLimit in
+/// `status` (when given) instead of spinning.
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, uint32_t n, int* status) {
+    for (uint32_t it = 0; it <= n; ++it) {
         const uint32_t p = __ldcg(parent + x);
         if (p == x) return x;
         const uint32_t gp = __ldcg(parent + p);
@@ -125,14 +128,16 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
         parent[x] = gp;  // halving; benign race
         x = gp;
     }
+    if (status) atomicOr(status, kStatusUnionLimit);
+    return x;
 }
 
 /// Unite the sets of a and b.  Returns true when this call linked two roots.
 /// The CAS retry loop is bounded; running out sets kStatusUnionLimit.
-__device__ __forceinline__ bool uf_unite(uint32_t* parent, uint32_t a, uint32_t b, int* status) {
+__device__ __forceinline__ bool uf_unite(uint32_t* parent, uint32_t a, uint32_t b, uint32_t n, int* status) {
     for (int it = 0; it < (1 << 20); ++it) {
-        a = uf_find(parent, a);
-        b = uf_find(parent, b);
+        a = uf_find(parent, a, n, status);
+        b = uf_find(parent, b, n, status);
         if (a == b) return false;
         if (a > b) {
             const uint32_t t = a;

@@ -47,6 +47,7 @@ struct MstView {
     unsigned long long* bins;
     uint32_t* ctr;  // [0] wc0 [1] wc1 [2] tc0 [3] tc1
     const float* core;
+    uint32_t n;     // nodes (bounds every union-find chase)
 };
 
 namespace {
@@ -80,8 +81,8 @@ __device__ __forceinline__ void edge_step(const MstView& m, uint32_t i, bool val
     uint32_t cu = 0, cv = 0;
     if (valid && u < n && v < n) {
         if (kReweight) w = max_ref(w, max_ref(__ldg(m.core + u), __ldg(m.core + v)));
-        cu = uf_find(m.parent, u);
-        cv = uf_find(m.parent, v);
+        cu = uf_find(m.parent, u, n, nullptr);
+        cv = uf_find(m.parent, v, n, nullptr);
         live = cu != cv;
         if (live) {
             const unsigned long long key = pack_key(w, i);
@@ -114,7 +115,7 @@ __device__ __forceinline__ void root_step(const MstView& m, uint32_t c, const ui
     const uint32_t old = atomicOr(m.bitmap + (i >> 5), bit);
     if (!(old & bit)) {
         atomicAdd(sbins + bin_of(bits), static_cast<unsigned long long>(mant_of(bits)));
-        uf_unite(m.parent, __ldg(eu + i), __ldg(ev + i), status);
+        uf_unite(m.parent, __ldg(eu + i), __ldg(ev + i), m.n, status);
     }
 }
 
@@ -196,7 +197,7 @@ __global__ void k_label_roots(uint32_t* __restrict__ parent_all, uint32_t n, uin
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     bool root = false;
     if (v < n) {
-        const uint32_t r = uf_find(parent, v);
+        const uint32_t r = uf_find(parent, v, n, nullptr);
         lab_all[static_cast<uint64_t>(j) * n + v] = r;
         root = r == v;
     }
@@ -471,6 +472,7 @@ void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_la
     m.bins = bins.as<unsigned long long>();
     m.ctr = ctr.as<uint32_t>();
     m.core = nullptr;
+    m.n = static_cast<uint32_t>(n);
     const unsigned grid_cap = static_cast<unsigned>(c.sm_count) * 8u;
     uint32_t in_count = static_cast<uint32_t>(E);
     uint32_t hc[4];
@@ -664,6 +666,7 @@ extern "C" cs_status cs_mst_noalloc(const uint32_t* d_u, const uint32_t* d_v, co
         mv.bins = cv.take<unsigned long long>(256);
         mv.ctr = cv.take<uint32_t>(16);
         mv.core = nullptr;
+        mv.n = static_cast<uint32_t>(n);
         int* status = cv.take<int>(16);
         unsigned long long* counts = cv.take<unsigned long long>(8);
         uint32_t* tiles = cv.take<uint32_t>(static_cast<uint64_t>(nbl) + ntl + 2);

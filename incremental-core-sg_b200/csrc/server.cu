@@ -54,7 +54,7 @@ __global__ void k_cut_unite(const cs_edge* __restrict__ tree, const unsigned lon
     const uint64_t x = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (x >= cap || x >= *count) return;
     const cs_edge e = tree[x];
-    if (static_cast<double>(e.w) <= eps) uf_unite(parent, e.u, e.v, status);
+    if (static_cast<double>(e.w) <= eps) uf_unite(parent, e.u, e.v, static_cast<uint32_t>(cap + 1), status);
 }
 
 struct Slot {

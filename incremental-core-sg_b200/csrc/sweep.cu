@@ -94,9 +94,11 @@ struct SweepArgs {
     unsigned long long* trace;  // [kMaxRounds][kTraceWords] per-round timestamps and sizes
 };
 
-/// find with path halving on forest j of the node-major parent array.
-__device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_t j) {
-    for (;;) {
+/// find with path halving on forest j of the node-major parent array.  A forest of n
+/// nodes has no chain longer than n; a chase that takes more steps (a cycle, which the
+/// linking rule rules out) sets the status and stops instead of spinning.
+__device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_t j, uint32_t n, int* status) {
+    for (uint32_t it = 0; it <= n; ++it) {
         const uint32_t p = __ldcg(parent + static_cast<uint64_t>(x) * kLanes + j);
         if (p == x) return x;
         const uint32_t gp = __ldcg(parent + static_cast<uint64_t>(p) * kLanes + j);
@@ -104,24 +106,29 @@ __device__ __forceinline__ uint32_t find32(uint32_t* parent, uint32_t x, uint32_
         parent[static_cast<uint64_t>(x) * kLanes + j] = gp;
         x = gp;
     }
+    atomicOr(status, kStatusUnionLimit);
+    return x;
 }
 
 /// Root of x in forest j without writing: the flatten passes use it, so that every
 /// entry a flatten writes is its own node's, and only ever the final root (path
 /// halving there would race with other nodes' flatten writes and could put back a
 /// stale intermediate ancestor after the root was written).
-__device__ __forceinline__ uint32_t root32(const uint32_t* parent, uint32_t x, uint32_t j) {
-    for (;;) {
+__device__ __forceinline__ uint32_t root32(const uint32_t* parent, uint32_t x, uint32_t j, uint32_t n, int* status) {
+    for (uint32_t it = 0; it <= n; ++it) {
         const uint32_t p = __ldcg(parent + static_cast<uint64_t>(x) * kLanes + j);
         if (p == x) return x;
         x = p;
     }
+    atomicOr(status, kStatusUnionLimit);
+    return x;
 }
 
-__device__ __forceinline__ bool unite32(uint32_t* parent, uint32_t a, uint32_t b, uint32_t j, int* status) {
+__device__ __forceinline__ bool unite32(uint32_t* parent, uint32_t a, uint32_t b, uint32_t j, uint32_t n,
+                                        int* status) {
     for (int it = 0; it < (1 << 20); ++it) {
-        a = find32(parent, a, j);
-        b = find32(parent, b, j);
+        a = find32(parent, a, j, n, status);
+        b = find32(parent, b, j, n, status);
         if (a == b) return false;
         if (a > b) {
             const uint32_t t = a;
@@ -425,11 +432,11 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
 
 /// Point node c's entry of forest `lane` at its root, if it is not there already
 /// (only ever the final root is written, so concurrent chases stay correct).
-__device__ __forceinline__ void point_at_root(uint32_t* parent, uint32_t c, unsigned lane) {
+__device__ __forceinline__ void point_at_root(uint32_t* parent, uint32_t c, unsigned lane, uint32_t n, int* status) {
     uint32_t* const pc = parent + static_cast<uint64_t>(c) * kLanes + lane;
     const uint32_t p = __ldcg(pc);
     if (p == c) return;
-    const uint32_t f = root32(parent, p, lane);
+    const uint32_t f = root32(parent, p, lane, n, status);
     if (f != p) *pc = f;
 }
 
@@ -496,7 +503,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                         *slot = kNoKey;
                         const uint32_t i = static_cast<uint32_t>(key);
                         const uint32_t bit = 1u << lane;
-                        if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.status);
+                        if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.n, a.status);
                     }
                 }
                 chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
@@ -514,7 +521,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             const uint32_t cnt = r == 0 ? a.n : __ldcg(a.ctr + (r == 1 ? 2 + par : 7));
             const uint32_t* lst = r == 1 ? a.rlist + static_cast<uint64_t>(par) * a.n : a.fl;
             for (uint32_t t = gw; t < cnt; t += nw) {
-                if (act) point_at_root(a.parent, r == 0 ? t : __ldcg(lst + t), lane);
+                if (act) point_at_root(a.parent, r == 0 ? t : __ldcg(lst + t), lane, a.n, a.status);
             }
             if (r == 1) {
                 const uint32_t nc = __ldcg(a.ctr + 2 + nxt);
@@ -560,7 +567,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     }
     // final flatten: parent[v][j] = root (the component's smallest node)
     for (uint32_t v = gw; v < a.n; v += nw) {
-        if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane);
+        if (act) a.parent[static_cast<uint64_t>(v) * kLanes + lane] = root32(a.parent, v, lane, a.n, a.status);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[4] = static_cast<uint32_t>(r + 1);
 }
