@@ -126,8 +126,9 @@ struct Server {
     /// A slot for `n` nodes, or null when none is free and memory does not admit a
     /// new one (the caller waits for the batches in flight).  Under mu.
     Slot* try_slot(uint64_t n) {
-        // a free slot that holds n nodes is reused as it is: slots are sized with a
-        // quarter of headroom, so a graph that grows by inserts keeps its slots
+        // a free slot that holds n nodes is reused as it is: slots are sized for the
+        // graph's capacity (cs_graph_reserve) or with a quarter of headroom, so a graph
+        // that grows by inserts keeps its slots
         for (size_t i = 0; i < free_slots.size(); ++i) {
             if (free_slots[i]->n >= n) {
                 Slot* s = free_slots[i];
@@ -142,7 +143,7 @@ struct Server {
         }
         free_slots.clear();
         if (all_slots.size() >= cfg.max_slots) return nullptr;
-        const uint64_t cap = n + n / 4;
+        const uint64_t cap = std::max<uint64_t>(n + n / 4, scratch_nodes(*g));
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return nullptr;
         const size_t need = slot_bytes_for(cap);
