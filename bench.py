@@ -531,6 +531,10 @@ def main():
                 "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes": kb, "kernel_ms": kernel_ms,
                 "traffic": prof[0] if prof else None,
                 "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/{prof[1]}" if prof else None,
+                # the bytes the kernel actually moves (every round re-reads the live edges)
+                # over its time, against the same peak
+                "traffic_gbs": prof[0] / (kernel_ms / 1000.0) / 1e9 if prof else None,
+                "traffic_frac": prof[0] / (kernel_ms / 1000.0) / 1e9 / peak if prof else None,
                 "sweep_graph": {"algorithmic_bytes": sweep_bytes(n, E, K), "ms": ms_per_step,
                                 "achieved_gbs": sweep_bytes(n, E, K) / (ms_per_step / 1000.0) / 1e9}}
 
