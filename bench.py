@@ -381,7 +381,9 @@ def run_serving(cs, ctx, args):
         "p50_insert_ms": percentile(ilat, 50), "p99_insert_ms": percentile(ilat, 99),
         "p50_ms": percentile(qlat + ilat, 50), "p99_ms": percentile(qlat + ilat, 99),
         "msts_per_s": len(qlat) / drain if drain > 0 else None, "drain_s": drain,
-        "sweeps": st["batches"], "mean_batch": (st["queries"] / st["batches"]) if st["batches"] else None,
+        "sweeps": st["batches"], "batches_from_last_sweep": st["reused_batches"],
+        "mean_batch": (st["queries"] / (st["batches"] + st["reused_batches"]))
+        if st["batches"] + st["reused_batches"] else None,
         "max_batch": st["max_batch_seen"], "insert_batches": st["insert_batches"],
         "inserted_rows": st["inserted_rows"], "sweep_ms_total": st["sweep_ms"], "insert_ms_total": st["insert_ms"],
         "result_buffers": args.serve_buffers, "result": "extract: tree edges; epsilon-cut: labels (pinned host)",

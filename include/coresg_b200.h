@@ -374,6 +374,8 @@ typedef struct {
     uint32_t max_batch_seen;   /* most requests served by one sweep */
     double sweep_ms;           /* device time of all sweeps */
     double insert_ms;          /* host time of all inserts */
+    uint64_t reused_batches;   /* query batches served from the last sweep of every mpts
+                                  (no insert since): no sweep run for them */
 } cs_server_stats;
 
 cs_status cs_server_create(cs_graph* g, const cs_server_config* cfg, cs_server** out);

@@ -39,7 +39,7 @@ class Stats(C.Structure):
                 ("batches", C.c_uint64), ("queries", C.c_uint64), ("inserts", C.c_uint64),
                 ("inserted_rows", C.c_uint64), ("insert_batches", C.c_uint64), ("slots", C.c_uint64),
                 ("slot_bytes", C.c_uint64), ("max_batch_seen", C.c_uint32), ("sweep_ms", C.c_double),
-                ("insert_ms", C.c_double)]
+                ("insert_ms", C.c_double), ("reused_batches", C.c_uint64)]
 
 
 class Pinned:

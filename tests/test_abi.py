@@ -48,7 +48,7 @@ def test_server_structs_match_the_header_layout():
     assert C.sizeof(Request) == 72 and Request.eps.offset == 8 and Request.out_labels_cap.offset == 64
     assert C.sizeof(Result) == 216 and Result.weight.offset == 24 and Result.error.offset == 56
     assert C.sizeof(ServerConfig) == 104 and ServerConfig.insert.offset == 24
-    assert C.sizeof(Stats) == 104 and Stats.sweep_ms.offset == 88
+    assert C.sizeof(Stats) == 112 and Stats.sweep_ms.offset == 88 and Stats.reused_batches.offset == 104
 
 
 def test_request_stream_is_seeded_and_shaped():

@@ -199,3 +199,43 @@ def test_back_to_back_inserts_coalesce_and_inserts_first(gpu_ctx):
         assert r["n"] in (n0, n1)
         assert e[: r["nedges"]].tobytes() == want.edges.tobytes()
         assert np.array_equal(lab[: r["n"]], want.component) and r["weight"] == want.weight
+
+
+def test_batches_between_inserts_reuse_the_last_sweep(gpu_ctx):
+    """With k_max <= 32 a sweep solves every mpts; later batches with no insert in
+    between are served from its results (no sweep), and after an insert the next batch
+    sweeps again.  Every result equals the request served alone on its graph state."""
+    z = load_golden("coresg_n3000_d24_k16")
+    g = resident(gpu_ctx, z)
+    n0 = len(z["counts"])
+    alone = {m: g.mst(m) for m in (1, 3, 8, 16)}
+    eps = float(np.quantile(alone[8].edges["w"], 0.6))
+    srv = cs.Server(g, max_batch=32)
+    # first batch: a sweep
+    e, lab = bufs(n0)
+    r = srv.wait(srv.extract(3, e, lab))
+    assert r["status"] == 0 and e[: r["nedges"]].tobytes() == alone[3].edges.tobytes()
+    sweeps = srv.stats()["batches"]
+    # more batches, nothing inserted: served from that sweep
+    for m in (16, 1, 8):
+        e, lab = bufs(n0)
+        r = srv.wait(srv.extract(m, e, lab))
+        assert r["status"] == 0 and e[: r["nedges"]].tobytes() == alone[m].edges.tobytes()
+        assert np.array_equal(lab[:n0], alone[m].component) and r["weight"] == alone[m].weight
+    cl = np.zeros(n0, np.uint32)
+    r = srv.wait(srv.cut(8, eps, cl))
+    want, k = cut_labels(alone[8].edges, n0, eps)
+    assert r["status"] == 0 and r["ncomp"] == k and np.array_equal(cl, want)
+    st = srv.stats()
+    assert st["batches"] == sweeps and st["reused_batches"] >= 4
+    # an insert: the next query sweeps the grown graph
+    rows = np.random.default_rng(9).normal(3.0, 1.0, size=(200, int(z["dim"]))).astype(np.float32)
+    assert srv.wait(srv.insert(rows))["status"] == 0
+    e, lab = bufs(n0 + len(rows))
+    r = srv.wait(srv.extract(8, e, lab))
+    st2 = srv.stats()
+    srv.close()
+    assert st2["batches"] == sweeps + 1
+    a = g.mst(8)
+    assert r["status"] == 0 and r["n"] == n0 + len(rows)
+    assert e[: r["nedges"]].tobytes() == a.edges.tobytes() and r["weight"] == a.weight
