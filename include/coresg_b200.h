@@ -304,8 +304,10 @@ cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint3
 /* A device-resident request loop over one cs_graph: extract(mpts) queries,
  * epsilon-cut label queries and insert batches are submitted from any host thread
  * and served in arrival order.  Consecutive queries are batched as they arrive:
- * every batch is one 32-lane graph-captured sweep over the distinct mpts it holds
- * (a query that arrives while a batch is on the GPU joins the next one), its
+ * every batch is one 32-lane graph-captured sweep (a query that arrives while a
+ * batch is on the GPU joins the next one) -- over every mpts 1..k_max when k_max <=
+ * 32, and then a later batch with no insert since is served from that sweep's
+ * results without a sweep; over the batch's distinct mpts otherwise -- its
  * results are copied into device result slots in stream order (one slot per
  * distinct extract mpts, shared by its queries, and one per epsilon-cut), and a
  * completion thread copies the slots into the callers' host buffers on a second
