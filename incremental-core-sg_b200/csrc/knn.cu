@@ -297,19 +297,42 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     }
     __syncwarp();
     // pairs: a in [0, nN) with every b > a in [0, nT) -- new x new once, new x old;
-    // row a is read by the whole warp at once (a broadcast), the lanes take the b's
+    // row a is read by the whole warp at once (a broadcast), the lanes take the b's.
+    // Every lane's offer to u1 goes to the same node: one atomicAdd reserves the
+    // warp's places in u1's append buffer (the lanes then fill them in lane order)
+    // instead of one contended atomic per lane.
     uint32_t my_evals = 0;
     for (uint32_t a = 0; a < nN; ++a) {
         const float* ra = s_row + static_cast<size_t>(a) * pitch;
         const uint32_t u1 = s_id[a];
         const float ta = s_thr[a];
-        for (uint32_t b = a + 1 + lane; b < nT; b += 32) {
-            const uint32_t u2 = s_id[b];
-            if (u1 == u2) continue;
-            const float r = l2sqr_ref(ra, s_row + static_cast<size_t>(b) * pitch, stride);
-            ++my_evals;
-            if (r < ta) offer(cand, u1, make_key(r, u2));
-            if (r < s_thr[b]) offer(cand, u2, make_key(r, u1));
+        for (uint32_t b0 = a + 1; b0 < nT; b0 += 32) {
+            const uint32_t b = b0 + lane;
+            const uint32_t u2 = b < nT ? s_id[b] : u1;
+            const bool pair = b < nT && u1 != u2;
+            float r = 0.0f;
+            if (pair) {
+                r = l2sqr_ref(ra, s_row + static_cast<size_t>(b) * pitch, stride);
+                ++my_evals;
+            }
+            const bool to1 = pair && r < ta;
+            const unsigned m1 = __ballot_sync(0xFFFFFFFFu, to1);
+            if (m1) {
+                uint32_t base = 0;
+                const unsigned leader = __ffs(m1) - 1;
+                if (lane == leader) base = atomicAdd(cand.cnt + u1, static_cast<uint32_t>(__popc(m1)));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (to1) {
+                    const uint32_t pos = base + __popc(m1 & ((1u << lane) - 1u));
+                    const unsigned long long key = make_key(r, u2);
+                    if (pos < kCap) {
+                        cand.buf[static_cast<uint64_t>(u1) * kCap + pos] = key;
+                    } else {
+                        offer_table(cand.table + static_cast<uint64_t>(u1) * kSlots, key);
+                    }
+                }
+            }
+            if (pair && r < s_thr[b]) offer(cand, u2, make_key(r, u1));
         }
     }
     if (evals) {
