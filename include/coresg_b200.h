@@ -89,6 +89,13 @@ void cs_ctx_destroy(cs_ctx* ctx);
 cs_status cs_ctx_trim(cs_ctx* ctx);
 /* Number of engine kernel launches issued on this context so far. */
 uint64_t cs_ctx_launches(const cs_ctx* ctx);
+/* Device allocations (cudaMalloc) the library has made in this process so far,
+ * and their bytes (freed buffers included).  After cs_graph_reserve(g, rows), an
+ * insert of any batch that keeps the graph within `rows` makes none, except when
+ * the k-NN graph then has more than 4x (+ 64) the components it had at the last
+ * bridge selection before the reserve, when the bridges leave components apart (the
+ * repair pass), or when the rows come with a stride above dim. */
+void cs_device_allocs(uint64_t* out_count, uint64_t* out_bytes);
 
 /* ---- the two device entry points the reference's CUDA backend binds -------- */
 
@@ -134,11 +141,11 @@ cs_status cs_graph_get_knn(cs_graph* g, uint32_t* ids, float* dists, uint8_t* fl
 cs_status cs_graph_set_bridges(cs_graph* g, const cs_edge* edges, uint64_t m);
 cs_status cs_graph_get_bridges(cs_graph* g, cs_edge* out, uint64_t cap, uint64_t* out_count);
 /* Capacity for `rows` nodes (Dataset::reserve, include/coresg/dataset.hpp:50): the
- * resident arrays and the node-proportional scratch of NN-Descent, inserts and the
- * bridge selection are allocated for that many nodes now, and the edge list and
- * sweep buffers are sized for it when next built, so inserts that stay within it
- * allocate no device memory (a fresh allocation of a few hundred MB took from a few
- * ms to over a second here).  Never shrinks. */
+ * resident arrays, the edge list, and the scratch of NN-Descent, inserts and the
+ * bridge selection are allocated for that many nodes now, and the sweep buffers are
+ * sized for it when next built, so inserts that stay within it allocate no device
+ * memory (cs_device_allocs states the exceptions; a fresh allocation of a few
+ * hundred MB took from a few ms to over a second here).  Never shrinks. */
 cs_status cs_graph_reserve(cs_graph* g, uint64_t rows);
 /* n, k_max, dim, stride, undirected k-NN edge count (KnnGraph::undirected_edge_count,
  * src/knn_graph.cpp:202-217), bridge count.  Any pointer may be NULL. */

@@ -47,6 +47,7 @@ _SIGS = {
     "cs_ctx_destroy": (None, [_p]),
     "cs_ctx_trim": (_i32, [_p]),
     "cs_ctx_launches": (_u64, [_p]),
+    "cs_device_allocs": (None, [_p, _p]),
     "cs_nndescent": (_i32, [_p, _p, _p, _p, _p, _p, _p, _p]),
     "cs_mrd_block": (_i32, [_p, _p, _sz, _u32, _u32, _i32, _p, _sz, _sz, _p]),
     "cs_graph_create": (_i32, [_p, _u32, _u32, _i32, _pp]),
@@ -98,6 +99,13 @@ def header_symbols(path: str = HEADER_PATH) -> list[str]:
     """Every function name declared in include/coresg_b200.h."""
     text = open(path).read()
     return sorted(set(re.findall(r"\b(cs_[a-z0-9_]+)\s*\(", text)))
+
+
+def device_allocs() -> tuple:
+    """(count, bytes) of the device allocations the library has made in this process."""
+    n, b = C.c_uint64(), C.c_uint64()
+    lib().cs_device_allocs(C.byref(n), C.byref(b))
+    return int(n.value), int(b.value)
 
 
 def write_edges_tsv(path, edges) -> None:

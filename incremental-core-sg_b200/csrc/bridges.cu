@@ -279,6 +279,23 @@ struct Scratch {
           pintree(g.bridge_scratch[20]), pout(g.bridge_scratch[21]), pcnt(g.bridge_scratch[22]) {}
 };
 
+/// The anti-hub budget: round(dim x ln |E|) with |E| the k-NN edge count, capped so
+/// the bridge MST's m^2 x dim / 2 coordinate operations stay within 2e9
+/// (m <= sqrt(4e9 / dim)), at least 2 and at most n (antihub_budget,
+/// src/hubness.cpp:16-40, with its default multiplier 1, max_pair_ops 2e9 and
+/// min_selected 2).
+uint64_t antihub_budget(uint64_t num_edges, uint32_t dim, uint64_t n) {
+    const double logs = num_edges > 1 ? std::log(static_cast<double>(num_edges)) : 0.0;
+    double raw = 1.0 * static_cast<double>(dim) * logs;
+    if (!(raw > 0.0)) raw = 0.0;
+    uint64_t budget = static_cast<uint64_t>(std::llround(raw));
+    const double m_max = std::sqrt(2.0 * 2e9 / static_cast<double>(dim));
+    if (m_max >= 1.0 && static_cast<double>(budget) > m_max) budget = static_cast<uint64_t>(m_max);
+    if (budget < 2) budget = 2;
+    if (budget > n) budget = n;
+    return budget;
+}
+
 /// The node-proportional selection scratch for `ns` nodes.
 void size_bridge_scratch(Scratch& s, uint64_t ns) {
     s.parent.ensure(ns * 4ull);
@@ -396,9 +413,37 @@ void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metri
     check_launch(c, "mrd rows");
 }
 
+uint64_t selection_bound(const Graph& g) {
+    const uint64_t ns = scratch_nodes(g);
+    return antihub_budget(ns * g.k, g.dim, ns) + 2 * (4ull * g.last_ncomp + 64) + 8;
+}
+
 void bridges_reserve(Graph& g) {
     Scratch s(g);
-    size_bridge_scratch(s, scratch_nodes(g));
+    const uint64_t ns = scratch_nodes(g);
+    size_bridge_scratch(s, ns);
+    // the rest of a selection on up to ns nodes: per-block label counts, the selected
+    // list, the per-component quota keys, the bridge MST over the selected nodes and
+    // the selection's sort keys
+    const uint64_t m = selection_bound(g), comps = 4ull * g.last_ncomp + 64;
+    const uint64_t md = std::min<uint64_t>(m, kDenseLimit);
+    s.bc.ensure(blocks_for(ns) * 4ull + 64);
+    s.ncomp.ensure(64);
+    s.hist.ensure(256 * 4);
+    s.sel.ensure(m * 4);
+    s.selcnt.ensure(64);
+    s.best_s.ensure(comps * 8);
+    s.best_t.ensure(comps * 8);
+    s.sub_pts.ensure(md * g.stride * 4);
+    s.sub_core.ensure(md * 4);
+    s.mat.ensure(md * md * 4);
+    s.pbest.ensure(md * 4);
+    s.pfrom.ensure(md * 4);
+    s.pintree.ensure(md + 16);
+    s.pout.ensure(md * sizeof(cs_edge) + 64);
+    s.pcnt.ensure(64);
+    g.ctx->scratch[6].ensure(m * 16 + 16);
+    g.bridges.grow_keep(md * sizeof(cs_edge), g.ctx->stream);
 }
 
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
@@ -443,19 +488,10 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     CSB_CUDA(cudaStreamSynchronize(c.stream));
     if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "connectivity: a union retry loop ran out");
     const uint32_t ncomp = static_cast<uint32_t>(ncomp64);
-    // ---- budget (host arithmetic identical to antihub_budget)
+    g.last_ncomp = ncomp;
+    // ---- budget
     graph_build_edges(g);
-    const uint64_t num_edges = g.e_knn;
-    const double logs = num_edges > 1 ? std::log(static_cast<double>(num_edges)) : 0.0;
-    double raw = 1.0 * static_cast<double>(g.dim) * logs;
-    if (!(raw > 0.0)) raw = 0.0;
-    uint64_t budget = static_cast<uint64_t>(std::llround(raw));
-    {
-        const double m_max = std::sqrt(2.0 * 2e9 / static_cast<double>(g.dim));
-        if (m_max >= 1.0 && static_cast<double>(budget) > m_max) budget = static_cast<uint64_t>(m_max);
-    }
-    if (budget < 2) budget = 2;
-    if (budget > n) budget = n;
+    const uint64_t budget = antihub_budget(g.e_knn, g.dim, n);
     // ---- selection: budget lowest under (score, rdeg, id)
     const uint32_t cap = static_cast<uint32_t>(budget + 2ull * ncomp + 8);
     s.hist.ensure(256 * 4);

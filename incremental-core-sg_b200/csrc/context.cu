@@ -1,5 +1,6 @@
 // Contexts, device query, error plumbing, device/pinned buffers and staging copies.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -10,7 +11,13 @@ namespace csb {
 
 namespace {
 thread_local std::string t_error;
+// device allocations made by DevBuf in this process: count and bytes
+std::atomic<uint64_t> g_dev_allocs{0}, g_dev_alloc_bytes{0};
+void count_alloc(size_t nbytes) {
+    g_dev_allocs.fetch_add(1, std::memory_order_relaxed);
+    g_dev_alloc_bytes.fetch_add(nbytes, std::memory_order_relaxed);
 }
+}  // namespace
 
 void set_thread_error(const std::string& m) { t_error = m; }
 const char* thread_error() { return t_error.c_str(); }
@@ -55,6 +62,7 @@ void DevBuf::ensure(size_t nbytes) {
         fail(CS_ERR_OOM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: " +
                              cudaGetErrorString(e));
     }
+    count_alloc(nbytes);
     p = q;
     bytes = nbytes;
 }
@@ -72,6 +80,7 @@ void DevBuf::grow_keep(size_t nbytes, cudaStream_t s) {
         CSB_CUDA(cudaMemcpyAsync(q, p, bytes, cudaMemcpyDeviceToDevice, s));
         CSB_CUDA(cudaStreamSynchronize(s));
     }
+    count_alloc(nbytes);
     release();
     p = q;
     bytes = nbytes;
@@ -311,6 +320,11 @@ cs_status cs_ctx_trim(cs_ctx* ctx) {
 uint64_t cs_ctx_launches(const cs_ctx* ctx) {
     const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
     return c ? c->launches : 0;
+}
+
+void cs_device_allocs(uint64_t* out_count, uint64_t* out_bytes) {
+    if (out_count) *out_count = g_dev_allocs.load(std::memory_order_relaxed);
+    if (out_bytes) *out_bytes = g_dev_alloc_bytes.load(std::memory_order_relaxed);
 }
 
 }  // extern "C"

@@ -129,8 +129,10 @@ struct Graph {
     uint64_t last_build_evals = 0;
     double last_build_ms = 0.0;
 
-    // Hubness selection of the last cs_select_bridges.
+    // Hubness selection of the last cs_select_bridges, and the component count of
+    // the k-NN graph it saw.
     std::vector<uint32_t> selected;
+    uint32_t last_ncomp = 0;
 
     // Batched sweep state (sweep.cu): a chain of plans, one per pass of <= 32 MSTs.
     SweepPlan* plan = nullptr;
@@ -159,6 +161,9 @@ inline uint64_t scratch_scale(const Graph& g, uint64_t count) {
 
 // graph.cu
 void graph_build_edges(Graph& g);  // cached base edge list (no-op when valid)
+/// Allocate the cached edge list and its enumeration scratch for scratch_nodes(g)
+/// nodes now.
+void edges_reserve(Graph& g);
 /// Upload (or append) n rows of `row_stride` floats as padded points; new nodes
 /// start with empty k-NN lists (Dataset::append + KnnGraph::grow).
 void graph_set_points(Graph& g, const float* rows, uint64_t n, uint32_t row_stride, bool append);
@@ -211,6 +216,9 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
 // bridges.cu
 /// Allocate the selection scratch for scratch_nodes(g) nodes now.
 void bridges_reserve(Graph& g);
+/// An upper bound of the selection size on a graph of up to scratch_nodes(g) nodes
+/// whose k-NN graph has at most 4x the last seen component count (+ 64).
+uint64_t selection_bound(const Graph& g);
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
                     uint32_t* out_components);
 void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metric,
@@ -219,6 +227,8 @@ void mrd_rows(Ctx& c, const float* d_pts, uint32_t m, uint32_t stride, int metri
 // scan.cu
 /// Exclusive prefix sum of n u32 values into out (n+1 entries; out[n] = total).
 void scan_u32(Ctx& c, const uint32_t* in, uint32_t* out, uint64_t n);
+/// Allocate scan_u32's scratch for scans of up to n items now.
+void scan_reserve(Ctx& c, uint64_t n);
 
 // host <-> device through the context's pinned staging (context.cu)
 void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes);

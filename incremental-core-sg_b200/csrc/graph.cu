@@ -192,8 +192,8 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
     const uint64_t total = static_cast<uint64_t>(e_knn) + g.nb;
     if (total > 0xFFFFFFFEull) fail(CS_ERR_UNSUPPORTED, "edge count exceeds 32-bit edge indices");
     // the graph's cached edge list is sized for its capacity (it is rebuilt after
-    // every insert)
-    const uint64_t room = &u == &g.eu ? std::max(scratch_scale(g, total), total) : total;
+    // every insert): the k-NN edges scaled to it, and the bridges
+    const uint64_t room = &u == &g.eu ? std::max(scratch_scale(g, e_knn) + g.nb, total) : total;
     u.ensure(room * sizeof(uint32_t) + 4);
     v.ensure(room * sizeof(uint32_t) + 4);
     w.ensure(room * sizeof(float) + 4);
@@ -212,6 +212,23 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
     }
     check_launch(c, "edge enumeration");
     return total;
+}
+
+void edges_reserve(Graph& g) {
+    Ctx& c = *g.ctx;
+    const uint64_t ns = scratch_nodes(g), words = (g.k + 31) / 32;
+    c.scratch[0].ensure(ns * words * sizeof(uint32_t) + 4);
+    c.scratch[1].ensure((ns + 1) * sizeof(uint32_t));
+    // the cached list: at most k edges per node, and the bridges; growing it drops
+    // the cached edges, which are enumerated again when next needed
+    const uint64_t room = ns * g.k + selection_bound(g);
+    if (g.node_off.bytes < (ns + 1) * sizeof(uint32_t) || g.eu.bytes < room * sizeof(uint32_t) + 4) {
+        g.node_off.ensure((ns + 1) * sizeof(uint32_t));
+        g.eu.ensure(room * sizeof(uint32_t) + 4);
+        g.ev.ensure(room * sizeof(uint32_t) + 4);
+        g.ew.ensure(room * sizeof(float) + 4);
+        g.invalidate_edges();
+    }
 }
 
 void graph_build_edges(Graph& g) {
@@ -458,6 +475,7 @@ cs_status cs_graph_reserve(cs_graph* gp, uint64_t rows) {
         if (rows > g->cap_n) g->ensure_capacity(rows, true);
         knn_reserve(*g);
         bridges_reserve(*g);
+        edges_reserve(*g);
     });
 }
 

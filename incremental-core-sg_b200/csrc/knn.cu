@@ -980,8 +980,28 @@ uint32_t expand_ring(Ctx& c, Graph& g, const uint32_t* src, uint32_t ns, uint8_t
 
 void knn_reserve(Graph& g) {
     KnnScratch s(g);
-    size_descent_scratch(s, scratch_nodes(g));
-    size_insert_scratch(g, scratch_nodes(g));
+    Ctx& c = *g.ctx;
+    const uint64_t ns = scratch_nodes(g), nk = ns * g.k;
+    size_descent_scratch(s, ns);
+    size_insert_scratch(g, ns);
+    // what an insert batch that keeps the graph within ns nodes needs besides: its
+    // seeds, the anti-hub entry points, the flags and offsets of its rings (at most ns
+    // nodes), the reverse index's sort and scan scratch, and the staged rows
+    const uint64_t rows = ns > g.n ? ns - g.n : 0;
+    const uint32_t width = std::min<uint32_t>(2 * g.k, 64);
+    g.insert_scratch[0].ensure(rows * width * 8);
+    g.insert_scratch[1].ensure(selection_bound(g) * 4);
+    g.insert_scratch[10].ensure(nk * 4 + 4);
+    g.insert_scratch[11].ensure(nk * 4 + 8);
+    if (nk < 0x7FFFFFFFull) {
+        // the widest sort (all 32 target bits) needs the most temporary storage
+        cub::DoubleBuffer<unsigned long long> db(nullptr, nullptr);
+        size_t tmp_bytes = 0;
+        CSB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, static_cast<int>(nk), 32, 64, c.stream));
+        g.insert_scratch[6].ensure(tmp_bytes + 16);
+    }
+    scan_reserve(c, nk);
+    c.scratch[6].ensure(rows * g.dim * 4);
 }
 
 void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride, const cs_insert_params& p,

@@ -91,6 +91,8 @@ __global__ void k_tile_apply(const uint32_t* __restrict__ in, uint64_t n,
 
 }  // namespace
 
+void scan_reserve(Ctx& c, uint64_t n) { c.scratch[7].ensure(((n + kTile - 1) / kTile + 2) * sizeof(uint64_t)); }
+
 void scan_u32(Ctx& c, const uint32_t* in, uint32_t* out, uint64_t n) {
     const uint64_t nb = (n + kTile - 1) / kTile;
     DevBuf& tmp = c.scratch[7];

@@ -70,3 +70,28 @@ def test_insert_requires_a_built_graph(gpu_ctx):
     g = cs.CoreSG(gpu_ctx, 8, 8)
     with pytest.raises(cs.CsError):
         g.insert(np.zeros((10, 8), np.float32))
+
+
+def test_inserts_within_a_reserve_allocate_nothing(gpu_ctx, oracle):
+    """cs_graph_reserve for every row to come, then inserts of four sizes (the largest
+    last): the library makes no device allocation during them (cs_device_allocs), and
+    the graph they leave keeps the KnnGraph invariants and carries the oracle's
+    bridges for it."""
+    k = 24
+    base, (old, fresh) = workload(seed=47, n=12000, batch=1500)
+    d = base.shape[1]
+    big = gaussian_mixture(4000, d, 4, (0.2, 1.0), 0.0, seed=101)
+    batches = [old[:200], old[200:], fresh, big]
+    g = cs.CoreSG(gpu_ctx, d, k)
+    g.build(base)
+    g.reserve(len(base) + sum(len(b) for b in batches))
+    before = cs.device_allocs()
+    for b in batches:
+        g.insert(b)
+    after = cs.device_allocs()
+    assert after == before, f"{after[0] - before[0]} device allocations ({after[1] - before[1]} bytes) in the inserts"
+    allpts = np.concatenate([base] + batches)
+    ids, dists, flags, counts = g.knn()
+    validate(ids, dists, counts, len(allpts), k)
+    br, _, _ = oracle.bridges(pad_rows(allpts), d, ids, dists, counts)
+    assert g.missing_edges().tobytes() == br.tobytes()
