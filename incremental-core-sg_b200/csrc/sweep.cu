@@ -661,11 +661,15 @@ __global__ void k_tree_count(const uint32_t* __restrict__ tree, uint32_t E, uint
     if (lane < K) tc[static_cast<uint64_t>(lane) * nchunks + chunk] = cnt;
 }
 
+/// Per-MST edge lists: chunk c of MST j starts at tc[j][c]; edges in ascending index.
+/// The MRD weight max(w, core_u, core_v) is taken from the sweep's core table (the
+/// value k_core32 wrote, so the weight is the one the sweep ranked): each edge reads
+/// the rows of its endpoints eight MSTs at a time (two 16-byte loads per row), all of
+/// a group's loads before its ballots.
 __global__ void k_tree_emit(const uint32_t* __restrict__ tree, uint32_t E, uint32_t K, uint32_t nchunks,
                             const uint32_t* __restrict__ tc, const uint32_t* __restrict__ eu,
                             const uint32_t* __restrict__ ev, const float* __restrict__ ew,
-                            const float* __restrict__ dists, const uint32_t* __restrict__ counts, uint32_t k,
-                            const uint32_t* __restrict__ mpts, uint64_t cap, cs_edge* __restrict__ out, int* status) {
+                            const float* __restrict__ core, uint64_t cap, cs_edge* __restrict__ out, int* status) {
     const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31u;
     if (chunk >= nchunks) return;
@@ -673,53 +677,80 @@ __global__ void k_tree_emit(const uint32_t* __restrict__ tree, uint32_t E, uint3
     for (uint32_t g = 0; g < kChunkEdges / 32; ++g) {
         const uint32_t i = chunk * kChunkEdges + g * 32 + lane;
         const uint32_t m = i < E ? tree[i] : 0u;
-        uint32_t u = 0, v = 0, cu = 0, cv = 0;
+        uint32_t u = 0, v = 0;
         float w = 0.0f;
         if (m) {
             u = eu[i];
             v = ev[i];
             w = ew[i];
-            cu = counts[u];
-            cv = counts[v];
         }
-        for (uint32_t j = 0; j < K; ++j) {
-            const bool has = (m >> j) & 1u;
-            const unsigned b = __ballot_sync(0xFFFFFFFFu, has);
-            if (!b) continue;
-            const uint32_t base = __shfl_sync(0xFFFFFFFFu, off, j);
-            if (has) {
-                const uint32_t mj = mpts[j];
-                const float inf = __int_as_float(0x7f800000);
-                const float c1 = cu ? dists[static_cast<uint64_t>(u) * k + (mj < cu ? mj : cu) - 1] : inf;
-                const float c2 = cv ? dists[static_cast<uint64_t>(v) * k + (mj < cv ? mj : cv) - 1] : inf;
-                const uint64_t pos = base + __popc(b & ((1u << lane) - 1u));
-                if (pos < cap) {
-                    cs_edge e;
-                    e.u = u;
-                    e.v = v;
-                    e.w = max_ref(w, max_ref(c1, c2));
-                    out[static_cast<uint64_t>(j) * cap + pos] = e;
-                } else {
-                    atomicOr(status, kStatusCapacity);
-                }
+        const float4* const ru = reinterpret_cast<const float4*>(core + static_cast<uint64_t>(u) * kLanes);
+        const float4* const rv = reinterpret_cast<const float4*>(core + static_cast<uint64_t>(v) * kLanes);
+        for (uint32_t j0 = 0; j0 < K; j0 += 8) {
+            const uint32_t mb = (m >> j0) & 0xFFu;
+            float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
+            if (mb) {
+                a0 = __ldg(ru + j0 / 4);
+                a1 = __ldg(ru + j0 / 4 + 1);
+                b0 = __ldg(rv + j0 / 4);
+                b1 = __ldg(rv + j0 / 4 + 1);
             }
-            if (lane == j) off += __popc(b);
+            const float cu[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float cv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+                const uint32_t j = j0 + x;  // < 32; bits at and above K are never set
+                const bool has = (mb >> x) & 1u;
+                const unsigned b = __ballot_sync(0xFFFFFFFFu, has);
+                if (!b) continue;
+                const uint32_t base = __shfl_sync(0xFFFFFFFFu, off, j);
+                if (has) {
+                    const uint64_t pos = base + __popc(b & ((1u << lane) - 1u));
+                    if (pos < cap) {
+                        cs_edge e;
+                        e.u = u;
+                        e.v = v;
+                        e.w = max_ref(w, max_ref(cu[x], cv[x]));
+                        out[static_cast<uint64_t>(j) * cap + pos] = e;
+                    } else {
+                        atomicOr(status, kStatusCapacity);
+                    }
+                }
+                if (lane == j) off += __popc(b);
+            }
         }
     }
 }
 
 /// Exact weight bins of each tree (per-exponent mantissa sums), one MST per block row.
+/// A warp's lanes of the same bin add their mantissas first (each < 2^24, so 32 of
+/// them fit 32 bits) and one lane adds the sum to the block's bin.
 __global__ void k_tree_weight(const cs_edge* __restrict__ out, uint64_t cap, const unsigned long long* __restrict__ nedges,
                               unsigned long long* __restrict__ bins) {
     __shared__ unsigned long long sb[256];
     const uint32_t j = blockIdx.y;
+    const unsigned lane = threadIdx.x & 31u;
     for (int b = threadIdx.x; b < 256; b += blockDim.x) sb[b] = 0;
     __syncthreads();
     const uint64_t ne = nedges[j] < cap ? nedges[j] : cap;
-    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < ne; t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t bits = __float_as_uint(out[static_cast<uint64_t>(j) * cap + t].w);
-        const uint32_t e = (bits >> 23) & 0xFFu;
-        atomicAdd(sb + (e ? e : 1u), static_cast<unsigned long long>((bits & 0x7FFFFFu) | (e ? 0x800000u : 0u)));
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    // whole warps step together, so the warp intrinsics see every lane of the warp
+    for (uint64_t t0 = static_cast<uint64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); t0 < ne; t0 += stride) {
+        const uint64_t t = t0 + lane;
+        const bool ok = t < ne;
+        uint32_t bin = 0, mant = 0;
+        if (ok) {
+            const uint32_t bits = __float_as_uint(out[static_cast<uint64_t>(j) * cap + t].w);
+            const uint32_t e = (bits >> 23) & 0xFFu;
+            bin = e ? e : 1u;
+            mant = (bits & 0x7FFFFFu) | (e ? 0x800000u : 0u);
+        }
+        const unsigned act = __ballot_sync(0xFFFFFFFFu, ok);
+        if (ok) {
+            const unsigned grp = __match_any_sync(act, bin);
+            const uint32_t sum = __reduce_add_sync(grp, mant);
+            if (lane == static_cast<unsigned>(__ffs(grp) - 1)) atomicAdd(sb + bin, static_cast<unsigned long long>(sum));
+        }
     }
     __syncthreads();
     for (int b = threadIdx.x; b < 256; b += blockDim.x) {
@@ -854,8 +885,7 @@ void enqueue_post(Graph& g, SweepPlan& p) {
     const uint64_t cap = p.n ? p.n - 1 : 0;
     k_tree_emit<<<ge, kThreads, 0, c.stream>>>(p.tree.as<uint32_t>(), p.E, p.K, p.nce, p.tcnt.as<uint32_t>(),
                                               g.eu.as<uint32_t>(), g.ev.as<uint32_t>(), g.ew.as<float>(),
-                                              g.dists.as<float>(), g.counts.as<uint32_t>(), g.k, p.mpts.as<uint32_t>(),
-                                              cap, p.out.as<cs_edge>(), p.status.as<int>());
+                                              p.core.as<float>(), cap, p.out.as<cs_edge>(), p.status.as<int>());
     dim3 gw(std::max<unsigned>(1, std::min<unsigned>(64, blocks_for(cap))), p.K);
     k_tree_weight<<<gw, kThreads, 0, c.stream>>>(p.out.as<cs_edge>(), cap, nedges, p.bins.as<unsigned long long>());
     count_launch(c, 2);
