@@ -225,6 +225,7 @@ __global__ void k_label_fill(const uint32_t* __restrict__ parent_all, uint32_t n
 
 /// Exclusive scan of `nt` u32 tile counts per MST (one block per MST); total -> tot[j].
 __global__ void k_scan_tiles(uint32_t* __restrict__ tiles, uint32_t nt, unsigned long long* __restrict__ tot) {
+    constexpr int kItems = 8;  // consecutive tiles per thread and pass
     const uint32_t j = blockIdx.x;
     uint32_t* t = tiles + static_cast<uint64_t>(j) * nt;
     __shared__ uint32_t wsum[32];
@@ -232,10 +233,15 @@ __global__ void k_scan_tiles(uint32_t* __restrict__ tiles, uint32_t nt, unsigned
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (uint32_t base = 0; base < nt; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t x = i < nt ? t[i] : 0u;
-        uint32_t incl = x;
+    for (uint32_t base = 0; base < nt; base += blockDim.x * kItems) {
+        const uint32_t first = base + threadIdx.x * kItems;
+        uint32_t x[kItems], sum = 0;
+#pragma unroll
+        for (int s = 0; s < kItems; ++s) {
+            x[s] = first + s < nt ? t[first + s] : 0u;
+            sum += x[s];
+        }
+        uint32_t incl = sum;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
             if (lane >= static_cast<unsigned>(o)) incl += y;
@@ -247,7 +253,12 @@ __global__ void k_scan_tiles(uint32_t* __restrict__ tiles, uint32_t nt, unsigned
             if (w < warp) before += wsum[w];
             all += wsum[w];
         }
-        if (i < nt) t[i] = carry + before + incl - x;
+        uint32_t run = carry + before + incl - sum;
+#pragma unroll
+        for (int s = 0; s < kItems; ++s) {
+            if (first + s < nt) t[first + s] = run;
+            run += x[s];
+        }
         __syncthreads();
         if (threadIdx.x == 0) carry += all;
         __syncthreads();

@@ -644,6 +644,8 @@ __global__ void k_lab_write(const uint32_t* __restrict__ parent, uint32_t n, uin
 
 // ---- trees: bit-packed membership -> per-MST edge lists in ascending edge index ----------
 
+/// tc[j][c] = edges of chunk c in MST j.  Lane j counts MST j: the warp walks only the
+/// group's edges that are in some tree (a few of 32), each one broadcast.
 __global__ void k_tree_count(const uint32_t* __restrict__ tree, uint32_t E, uint32_t K, uint32_t nchunks,
                              uint32_t* __restrict__ tc) {
     const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -653,9 +655,11 @@ __global__ void k_tree_count(const uint32_t* __restrict__ tree, uint32_t E, uint
     for (uint32_t g = 0; g < kChunkEdges / 32; ++g) {
         const uint32_t i = chunk * kChunkEdges + g * 32 + lane;
         const uint32_t m = i < E ? tree[i] : 0u;
-        for (uint32_t j = 0; j < K; ++j) {
-            const unsigned b = __ballot_sync(0xFFFFFFFFu, (m >> j) & 1u);
-            if (lane == j) cnt += __popc(b);
+        unsigned nz = __ballot_sync(0xFFFFFFFFu, m != 0u);
+        while (nz) {
+            const int t = __ffs(nz) - 1;
+            nz &= nz - 1;
+            cnt += (__shfl_sync(0xFFFFFFFFu, m, t) >> lane) & 1u;
         }
     }
     if (lane < K) tc[static_cast<uint64_t>(lane) * nchunks + chunk] = cnt;
