@@ -16,7 +16,9 @@ Reported (one JSON line from rank 0):
   build_s    device CORE-SG build: NN-Descent + anti-hub bridges, on a fresh graph (its
              device allocations included); rebuild_s the same build again on it
   e2e        the same metric through the C ABI with host buffers: the CORE-SG arrays
-             copied host->device and all K trees + labels copied back, every step
+             copied host->device and all K trees + labels copied back, every step;
+             two graphs in flight on their own contexts, so one step's copies overlap
+             the other's sweep (e2e.serial: one graph, steps back to back)
   roofline   the persistent Boruvka kernel against the measured HBM copy bandwidth
   cpu_baseline  the reference CPU extract (built from its sources) on the same
              CORE-SG, a bounded sample of mpts values, all host threads
@@ -292,6 +294,84 @@ def run_highdim(cs, ctx, args):
     return out
 
 
+def run_e2e(cs, ctx, g, mpts, arrays, steps, inflight, max_over_ranks, world, shape=None):
+    """The batched sweep through the C ABI with host buffers (`arrays`: the graph's
+    k-NN ids, dists, flags, counts and bridges).  A step is one
+    cs_graph_set_knn + cs_graph_set_bridges from page-locked host arrays and one
+    cs_extract_sweep into page-locked host outputs (all K trees and labels).
+    `inflight` graphs, each with its own context (stream) and a host thread, run
+    `steps` steps each, so one graph's uploads and downloads overlap another's sweep
+    (the copy engines and the SMs work at once); inflight = 1 is the plain serial loop.
+    Each graph runs one untimed step first (its plan is captured there).  Throughput
+    = all MSTs / the wall time of the region, max over ranks; `serial` is the same
+    loop with one graph.  `shape` (flatten divisor, block) is set on the added
+    graphs when the main one was given it; otherwise they take the autotuned shape
+    cached for this graph size."""
+    import threading
+
+    K, n = len(mpts), g.n
+
+    def pinned_copy(a):
+        p = cs.Pinned(a.shape, a.dtype)
+        p.array[...] = a
+        return p
+
+    host_in = [pinned_copy(a) for a in arrays]
+    p_ids, p_dists, p_flags, p_counts, p_bridges = (p.array for p in host_in)
+    h2d = sum(p.array.nbytes for p in host_in)
+    ctxs = [ctx] + [cs.Context(ctx.device) for _ in range(inflight - 1)]
+    graphs = [g] + [cs.CoreSG(c, g.dim, g.k_max) for c in ctxs[1:]]
+    if shape:
+        for gg in graphs[1:]:
+            gg.set_sweep_shape(*shape)
+    outs = [(cs.Pinned((K, max(n - 1, 1)), cs.EDGE_DTYPE), cs.Pinned((K, n), np.uint32)) for _ in graphs]
+    d2h = [0]
+
+    def step(w):
+        gg, (oe, ol) = graphs[w], outs[w]
+        gg.set_knn(p_ids, p_dists, p_flags, p_counts)
+        gg.set_bridges(p_bridges)
+        res = gg.all_msts(mpts, labels=True, out_edges=oe.array, out_labels=ol.array)
+        d2h[0] = sum(r.edges.nbytes + r.component.nbytes + 20 for r in res)
+
+    errors = []
+
+    def worker(w):
+        try:
+            for _ in range(steps):
+                step(w)
+        except Exception as ex:  # surfaced after the join
+            errors.append(repr(ex))
+
+    def timed(ws):
+        th = [threading.Thread(target=worker, args=(w,)) for w in ws]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return time.perf_counter() - t0
+
+    try:
+        for w in range(len(graphs)):
+            step(w)  # untimed: plan capture
+        serial_s = max_over_ranks(timed([0]))
+        piped_s = max_over_ranks(timed(range(len(graphs)))) if inflight > 1 else serial_s
+        if errors:
+            raise RuntimeError("e2e step failed: " + errors[0])
+    finally:
+        for p in host_in + [x for o in outs for x in o]:
+            p.free()
+        for gg in graphs[1:]:
+            gg.close()
+        for c in ctxs[1:]:
+            c.close()
+    return {"value": world * K * steps * len(graphs) / piped_s, "unit": "MSTs/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h[0]), "steps": steps * len(graphs), "inflight": len(graphs),
+            "serial": {"value": world * K * steps / serial_s, "steps": steps},
+            "what": f"cs_graph_set_knn + cs_graph_set_bridges + cs_extract_sweep (trees and labels) per step, page-locked host buffers; {len(graphs)} graph(s) on their own contexts in flight"}
+
+
 def run_serving(cs, ctx, args):
     """The serving workload: a resident CORE-SG of the serve workload, Poisson
     arrivals (extract(mpts ~ U{1..k_max}), a quarter of them epsilon-cuts at a random
@@ -398,7 +478,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blobs1m_d16")
     ap.add_argument("--n", type=int, default=None, help="override the workload's point count")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5, help="e2e steps per graph in flight (0: skip)")
+    ap.add_argument("--e2e-inflight", type=int, default=2, help="e2e graphs in flight, each on its own context")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--flatten", type=int, default=0, help="sweep flatten divisor (0: autotune)")
@@ -493,35 +574,15 @@ def main():
                  "kernel_launches": ctx.launches - ctx_l0,
                  "what": "cs_extract per mpts: edges(mpts) materialised, Boruvka rounds host-driven"}
 
-    # ---- e2e through the C ABI with host buffers: the CORE-SG's k-NN arrays and
-    # bridges in page-locked host memory go up, all K trees and labels come back into
-    # page-locked host arrays, every step
+    # ---- e2e through the C ABI with host buffers (run_e2e): every step uploads the
+    # CORE-SG's k-NN arrays and bridges and downloads all K trees and labels
     ids, dists, flags, counts = g.knn()
     bridges = g.missing_edges()
     e2e = None
     if args.e2e_steps > 0:
-        def pinned_copy(a):
-            p = cs.Pinned(a.shape, a.dtype)
-            p.array[...] = a
-            return p
-        host_in = [pinned_copy(a) for a in (ids, dists, flags, counts, bridges)]
-        p_ids, p_dists, p_flags, p_counts, p_bridges = (p.array for p in host_in)
-        out_e = cs.Pinned((K, max(n - 1, 1)), cs.EDGE_DTYPE)
-        out_l = cs.Pinned((K, n), np.uint32)
-        h2d = sum(p.array.nbytes for p in host_in)
-        secs, d2h = [], 0
-        for _ in range(args.e2e_steps):
-            t2 = time.perf_counter()
-            g.set_knn(p_ids, p_dists, p_flags, p_counts)
-            g.set_bridges(p_bridges)
-            res = g.all_msts(mpts, labels=True, out_edges=out_e.array, out_labels=out_l.array)
-            secs.append(time.perf_counter() - t2)
-            d2h = sum(r.edges.nbytes + r.component.nbytes + 20 for r in res)
-        for p in host_in + [out_e, out_l]:
-            p.free()
-        e2e_s = max_over_ranks(sum(secs))
-        e2e = {"value": world * K * len(secs) / e2e_s, "unit": "MSTs/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "steps": len(secs)}
+        shape = (args.flatten, args.block) if args.flatten and args.block else None
+        e2e = run_e2e(cs, ctx, g, mpts, (ids, dists, flags, counts, bridges), args.e2e_steps, args.e2e_inflight,
+                      max_over_ranks, world, shape)
 
     # ---- roofline of the persistent kernel
     peak, peak_kind = peaks()

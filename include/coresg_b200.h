@@ -272,7 +272,11 @@ cs_status cs_extract(cs_graph* g, uint32_t mpts, cs_edge* out_edges, uint32_t* o
  * pass of up to 32 MSTs (one warp lane per MST), replayed from CUDA graphs
  * (CoreSG::all_msts, src/coresg.cpp:412-417, which the reference runs as K
  * independent extractions).  Per-MST results as cs_extract, packed: out_edges
- * K*(n-1), out_labels K*n, and K-long count/weight arrays.  Any output may be NULL. */
+ * K*(n-1), out_labels K*n, and K-long count/weight arrays.  Any output may be NULL.
+ * Sweeps of all contexts on one device run one at a time (the persistent kernel
+ * takes every SM); the copies of the results to the host run outside that, so a
+ * host that keeps two graphs on two contexts in flight overlaps one graph's
+ * uploads and downloads with the other's sweep. */
 cs_status cs_extract_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, cs_edge* out_edges,
                            uint32_t* out_labels, uint64_t* out_nedges, uint32_t* out_ncomp,
                            double* out_weight);

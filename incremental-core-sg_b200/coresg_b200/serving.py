@@ -42,21 +42,16 @@ class Stats(C.Structure):
                 ("insert_ms", C.c_double), ("reused_batches", C.c_uint64)]
 
 
-class Pinned:
-    """A page-locked host array (cs_host_alloc); freed with free() or on collection."""
+class _HostMemory:
+    """Owns one cs_host_alloc block; frees it when collected or on free()."""
 
-    def __init__(self, shape, dtype):
-        dtype = np.dtype(dtype)
-        nbytes = int(np.prod(shape)) * dtype.itemsize
+    def __init__(self, nbytes: int):
         self.ptr = lib().cs_host_alloc(max(nbytes, 1))
         if not self.ptr:
             raise MemoryError("cs_host_alloc failed")
-        buf = (C.c_char * max(nbytes, 1)).from_address(self.ptr)
-        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
 
     def free(self):
         if self.ptr:
-            self.array = None
             lib().cs_host_free(self.ptr)
             self.ptr = None
 
@@ -65,6 +60,29 @@ class Pinned:
             self.free()
         except Exception:
             pass
+
+
+class Pinned:
+    """A page-locked host array (cs_host_alloc).  Every view of `array` keeps the
+    memory alive (so `Pinned(shape, dtype).array` alone is safe to hold); it is freed
+    once neither this object nor any view is referenced, or at once by free(), after
+    which no view may be used."""
+
+    def __init__(self, shape, dtype):
+        dtype = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dtype.itemsize
+        self._mem = _HostMemory(nbytes)
+        buf = (C.c_char * max(nbytes, 1)).from_address(self._mem.ptr)
+        buf._mem = self._mem  # numpy keeps buf alive for every view; buf keeps the memory
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    @property
+    def ptr(self):
+        return self._mem.ptr
+
+    def free(self):
+        self.array = None
+        self._mem.free()
 
 
 class Server:

@@ -796,6 +796,16 @@ void sweep_free(SweepPlan* p) { delete p; }
 namespace {
 
 std::mutex g_tune_mu;
+
+/// Sweeps on one device run one at a time, across contexts.  The persistent kernel
+/// takes every SM, so a second sweep in flight gains nothing; interleaved, each
+/// context's post-processing waited behind the other's whole kernel (two contexts'
+/// steps finished together, after both sweeps).  Serialised, one context's copies
+/// (its inputs going up, its trees coming down) overlap another context's sweep.
+std::mutex& device_sweep_mutex(int device) {
+    static std::mutex mus[64];
+    return mus[static_cast<unsigned>(device) % 64u];
+}
 std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, std::pair<uint32_t, uint32_t>> g_tuned;  // -> (block, flatten_div)
 
 SweepArgs args_of(Graph& g, SweepPlan& p) {
@@ -1052,8 +1062,9 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
         if (mpts[j] > g.k) fail(CS_ERR_INVALID, "sweep: mpts exceeds k_max");
     }
     if (g.n == 0) fail(CS_ERR_STATE, "sweep: empty graph");
-    graph_build_edges(g);
     Ctx& c = *g.ctx;
+    std::lock_guard<std::mutex> device_lock(device_sweep_mutex(c.device));
+    graph_build_edges(g);
     uint32_t B = g.sweep_block, F = g.sweep_flatten;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1106,7 +1117,8 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
         kms += x;
         status_check(c, p->status.as<int>());
         uint32_t rounds = 0;
-        CSB_CUDA(cudaMemcpy(&rounds, p->ctr.as<uint32_t>() + 4, 4, cudaMemcpyDeviceToHost));
+        CSB_CUDA(cudaMemcpyAsync(&rounds, p->ctr.as<uint32_t>() + 4, 4, cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
         p->last_rounds = rounds;
     }
     g.plan->last_graph_ms = ms;

@@ -79,6 +79,30 @@ def test_sweep_matches_reference(gpu_ctx, oracle, name, shape):
         check_tree(oracle, z, e, r, m, n)
 
 
+def test_pinned_views_keep_their_memory(gpu_ctx):
+    """A view of a Pinned array keeps the page-locked memory alive after the Pinned
+    object itself is dropped, and the memory is released once the last view goes."""
+    import gc
+    import weakref
+
+    p = cs.Pinned((4096,), np.uint32)
+    mem = weakref.ref(p._mem)
+    view = p.array[100:200]
+    del p
+    gc.collect()
+    assert mem() is not None and mem().ptr
+    view[:] = 7  # still mapped
+    assert int(view.sum()) == 700
+    del view
+    gc.collect()
+    assert mem() is None
+    # an explicit free releases the memory at once
+    q = cs.Pinned((16,), np.uint32)
+    m2 = q._mem
+    q.free()
+    assert m2.ptr is None and q.array is None
+
+
 def test_sweep_into_pinned_outputs(gpu_ctx):
     """Trees and labels written into caller-provided page-locked arrays (copied by DMA
     without staging) equal the ones returned in fresh pageable arrays, twice in a row,
