@@ -105,10 +105,14 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, folder=None):
+        """Samples go to `folder`/clocks_rank<device>.csv (a temporary folder when
+        None); the summary is what the JSON line carries."""
+        import tempfile
+
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.path = os.path.join(folder or tempfile.gettempdir(), f"clocks_rank{device}.csv")
 
     def start(self):
         try:
@@ -480,6 +484,7 @@ def main():
     ap.add_argument("--n", type=int, default=None, help="override the workload's point count")
     ap.add_argument("--e2e-steps", type=int, default=5, help="e2e steps per graph in flight (0: skip)")
     ap.add_argument("--e2e-inflight", type=int, default=2, help="e2e graphs in flight, each on its own context")
+    ap.add_argument("--clocks-dir", default=None, help="folder for the raw nvidia-smi samples (default: a temp folder)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--flatten", type=int, default=0, help="sweep flatten divisor (0: autotune)")
@@ -543,7 +548,7 @@ def main():
     log(f"[rank {rank}] sweep shape flatten_div={flatten} block={block}")
     for _ in range(args.warmup):
         g.sweep_device(mpts)
-    clk = Clocks(local)
+    clk = Clocks(local, args.clocks_dir)
     barrier()
     launches0 = ctx.launches
     clk.start()
