@@ -482,7 +482,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blobs1m_d16")
     ap.add_argument("--n", type=int, default=None, help="override the workload's point count")
-    ap.add_argument("--e2e-steps", type=int, default=5, help="e2e steps per graph in flight (0: skip)")
+    ap.add_argument("--e2e-steps", type=int, default=10, help="e2e steps per graph in flight (0: skip)")
     ap.add_argument("--e2e-inflight", type=int, default=2, help="e2e graphs in flight, each on its own context")
     ap.add_argument("--clocks-dir", default=None, help="folder for the raw nvidia-smi samples (default: a temp folder)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
