@@ -572,10 +572,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[4] = static_cast<uint32_t>(r + 1);
 }
 
-/// core[v][j] = core distance of v at mpts[j] (core_dist, include/coresg/knn_graph.hpp:157-163;
-/// +inf for an empty list); lanes >= K hold 0.
+/// The per-sweep node tables in one pass: core[v][j] = core distance of v at mpts[j]
+/// (core_dist, include/coresg/knn_graph.hpp:157-163; +inf for an empty list; lanes
+/// >= K hold 0), and parent[v][j] = v (every node its own root).
 __global__ void k_core32(const float* __restrict__ dists, const uint32_t* __restrict__ counts, uint32_t k,
-                         const uint32_t* __restrict__ mpts, uint32_t K, uint32_t n, float* __restrict__ core) {
+                         const uint32_t* __restrict__ mpts, uint32_t K, uint32_t n, float* __restrict__ core,
+                         uint32_t* __restrict__ parent) {
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= static_cast<uint64_t>(n) * kLanes) return;
     const uint32_t v = static_cast<uint32_t>(t / kLanes), j = static_cast<uint32_t>(t % kLanes);
@@ -585,11 +587,7 @@ __global__ void k_core32(const float* __restrict__ dists, const uint32_t* __rest
         x = c == 0 ? __int_as_float(0x7f800000) : dists[static_cast<uint64_t>(v) * k + (m < c ? m : c) - 1];
     }
     core[t] = x;
-}
-
-__global__ void k_identity32(uint32_t* __restrict__ parent, uint32_t n) {
-    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < static_cast<uint64_t>(n) * kLanes) parent[t] = static_cast<uint32_t>(t / kLanes);
+    parent[t] = v;
 }
 
 // ---- labels, numbered by each component's smallest node --------------------------------
@@ -690,7 +688,9 @@ __global__ void k_tree_emit(const uint32_t* __restrict__ tree, uint32_t E, uint3
         }
         const float4* const ru = reinterpret_cast<const float4*>(core + static_cast<uint64_t>(u) * kLanes);
         const float4* const rv = reinterpret_cast<const float4*>(core + static_cast<uint64_t>(v) * kLanes);
+        const unsigned any = __reduce_or_sync(0xFFFFFFFFu, m);  // MSTs some edge of the group is in
         for (uint32_t j0 = 0; j0 < K; j0 += 8) {
+            if (!((any >> j0) & 0xFFu)) continue;  // warp-uniform
             const uint32_t mb = (m >> j0) & 0xFFu;
             float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
             if (mb) {
@@ -704,6 +704,7 @@ __global__ void k_tree_emit(const uint32_t* __restrict__ tree, uint32_t E, uint3
 #pragma unroll
             for (int x = 0; x < 8; ++x) {
                 const uint32_t j = j0 + x;  // < 32; bits at and above K are never set
+                if (!((any >> j) & 1u)) continue;  // warp-uniform: no lane has the bit
                 const bool has = (mb >> x) & 1u;
                 const unsigned b = __ballot_sync(0xFFFFFFFFu, has);
                 if (!b) continue;
@@ -851,10 +852,10 @@ void enqueue_pre(Graph& g, SweepPlan& p) {
     CSB_CUDA(cudaMemsetAsync(p.tree.p, 0, E * 4, c.stream));
 
     CSB_CUDA(cudaMemsetAsync(p.bins.p, 0, static_cast<uint64_t>(p.K) * 256 * 8, c.stream));
-    k_identity32<<<blocks_for(n * kLanes), kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n);
     k_core32<<<blocks_for(n * kLanes), kThreads, 0, c.stream>>>(g.dists.as<float>(), g.counts.as<uint32_t>(), g.k,
-                                                                 p.mpts.as<uint32_t>(), p.K, p.n, p.core.as<float>());
-    count_launch(c, 2);
+                                                                 p.mpts.as<uint32_t>(), p.K, p.n, p.core.as<float>(),
+                                                                 p.parent.as<uint32_t>());
+    count_launch(c);
 }
 
 void enqueue_main(Graph& g, SweepPlan& p) {
@@ -934,7 +935,7 @@ bool capture_part(Graph& g, SweepPlan& p, Enqueue f, cudaGraphExec_t* out) {
     return ok;
 }
 
-uint64_t kernels_pre() { return 2; }
+uint64_t kernels_pre() { return 1; }
 uint64_t kernels_post(const SweepPlan& p) { return (p.labels ? 4 : 0) + 4; }
 
 /// A plan for the graph's current shape.  `reuse` (a plan that no longer matches)
