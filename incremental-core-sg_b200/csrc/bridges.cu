@@ -195,26 +195,26 @@ __global__ void k_mrd(const float* __restrict__ pts, uint32_t m, uint32_t stride
 /// Prim over the dense matrix in one CTA (mst_prim_virtual, src/mst.cpp:274-330):
 /// start at 0, relax from the current row, pick the smallest best[] with the lowest
 /// index winning ties; edges carry the base distance of their endpoints
-/// (src/coresg.cpp:346-351) and global ids via `ids`.
+/// (src/coresg.cpp:346-351) and global ids via `ids`.  The frontier (best, from,
+/// in-tree: 9 bytes per node) lives in shared memory; a step's pick is one warp's
+/// reduction of the warps' minima; the edges are recorded as local (from, pick) pairs
+/// in pick order and their base distances computed by all threads after the loop.
 __global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* __restrict__ pts, uint32_t stride,
-                       int metric, const uint32_t* __restrict__ ids, float* __restrict__ best, uint32_t* __restrict__ from,
-                       uint8_t* __restrict__ in_tree, cs_edge* __restrict__ out, uint32_t* __restrict__ out_count) {
-    __shared__ unsigned long long red[1024 / 32];
-    __shared__ uint32_t s_pick;
-    __shared__ float s_pick_w;
-    __shared__ uint32_t s_cnt;
+                       int metric, const uint32_t* __restrict__ ids, cs_edge* __restrict__ out,
+                       uint32_t* __restrict__ out_count) {
+    extern __shared__ unsigned char prim_smem[];
+    float* const best = reinterpret_cast<float*>(prim_smem);
+    uint32_t* const from = reinterpret_cast<uint32_t*>(best + m);
+    uint8_t* const in_tree = reinterpret_cast<uint8_t*>(from + m);
+    __shared__ unsigned long long red[32];
+    __shared__ uint32_t s_pick, s_cnt;
     const float inf = __int_as_float(0x7f800000);
     for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
-        best[j] = inf;
+        best[j] = j == 0 ? 0.0f : inf;
         from[j] = kInvalid;
-        in_tree[j] = 0;
+        in_tree[j] = j == 0 ? 1 : 0;
     }
     if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        in_tree[0] = 1;
-        best[0] = 0.0f;
-    }
     __syncthreads();
     uint32_t current = 0;
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -226,11 +226,13 @@ __global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* _
         for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
             if (in_tree[j]) continue;
             const float w = row[j];
-            if (w < best[j]) {
+            float b = best[j];
+            if (w < b) {
+                b = w;
                 best[j] = w;
                 from[j] = current;
             }
-            const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(best[j])) << 32) | j;
+            const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(b)) << 32) | j;
             mine = key < mine ? key : mine;
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -239,22 +241,22 @@ __global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* _
         }
         if (lane == 0) red[warp] = mine;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long b = kNoKey;
-            for (unsigned w2 = 0; w2 < nw; ++w2) b = red[w2] < b ? red[w2] : b;
-            s_pick = b == kNoKey ? kInvalid : static_cast<uint32_t>(b);
-            s_pick_w = b == kNoKey ? inf : __uint_as_float(static_cast<uint32_t>(b >> 32));
-            if (s_pick != kInvalid) {
-                in_tree[s_pick] = 1;
-                if (from[s_pick] != kInvalid && s_pick_w < inf) {
-                    const uint32_t a = from[s_pick], bb = s_pick;
-                    const float base = finalize_rank(l2sqr_ref(pts + static_cast<uint64_t>(a) * stride, pts + static_cast<uint64_t>(bb) * stride, stride), metric);
-                    const uint32_t ga = ids[a], gb = ids[bb];
-                    cs_edge e;
-                    e.u = ga < gb ? ga : gb;
-                    e.v = ga < gb ? gb : ga;
-                    e.w = base;
-                    out[s_cnt++] = e;
+        if (warp == 0) {
+            unsigned long long v = lane < nw ? red[lane] : kNoKey;
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                v = other < v ? other : v;
+            }
+            if (lane == 0) {
+                const uint32_t pick = v == kNoKey ? kInvalid : static_cast<uint32_t>(v);
+                s_pick = pick;
+                if (pick != kInvalid) {
+                    in_tree[pick] = 1;
+                    if (from[pick] != kInvalid && __uint_as_float(static_cast<uint32_t>(v >> 32)) < inf) {
+                        out[s_cnt].u = from[pick];  // local indices until the pass below
+                        out[s_cnt].v = pick;
+                        ++s_cnt;
+                    }
                 }
             }
         }
@@ -262,21 +264,32 @@ __global__ void k_prim(const float* __restrict__ mat, uint32_t m, const float* _
         if (s_pick == kInvalid) break;
         current = s_pick;
     }
-    if (threadIdx.x == 0) *out_count = s_cnt;
+    __syncthreads();
+    const uint32_t cnt = s_cnt;
+    for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const uint32_t a = out[t].u, bb = out[t].v;
+        const float base = finalize_rank(l2sqr_ref(pts + static_cast<uint64_t>(a) * stride, pts + static_cast<uint64_t>(bb) * stride, stride), metric);
+        const uint32_t ga = ids[a], gb = ids[bb];
+        cs_edge e;
+        e.u = ga < gb ? ga : gb;
+        e.v = ga < gb ? gb : ga;
+        e.w = base;
+        out[t] = e;
+    }
+    if (threadIdx.x == 0) *out_count = cnt;
 }
 
 /// Views of the graph's cached selection scratch (grow-only buffers).
 struct Scratch {
     DevBuf &parent, &lab, &bc, &ncomp, &rdeg, &score, &ks, &kt, &hist, &chosen, &qtaken, &sel, &selcnt, &best_s,
-        &best_t, &sub_pts, &sub_core, &mat, &pbest, &pfrom, &pintree, &pout, &pcnt;
+        &best_t, &sub_pts, &sub_core, &mat, &pout, &pcnt;
     explicit Scratch(Graph& g)
         : parent(g.bridge_scratch[0]), lab(g.bridge_scratch[1]), bc(g.bridge_scratch[2]), ncomp(g.bridge_scratch[3]),
           rdeg(g.bridge_scratch[4]), score(g.bridge_scratch[5]), ks(g.bridge_scratch[6]), kt(g.bridge_scratch[7]),
           hist(g.bridge_scratch[8]), chosen(g.bridge_scratch[9]), qtaken(g.bridge_scratch[10]),
           sel(g.bridge_scratch[11]), selcnt(g.bridge_scratch[12]), best_s(g.bridge_scratch[13]),
           best_t(g.bridge_scratch[14]), sub_pts(g.bridge_scratch[15]), sub_core(g.bridge_scratch[16]),
-          mat(g.bridge_scratch[17]), pbest(g.bridge_scratch[18]), pfrom(g.bridge_scratch[19]),
-          pintree(g.bridge_scratch[20]), pout(g.bridge_scratch[21]), pcnt(g.bridge_scratch[22]) {}
+          mat(g.bridge_scratch[17]), pout(g.bridge_scratch[21]), pcnt(g.bridge_scratch[22]) {}
 };
 
 /// The anti-hub budget: round(dim x ln |E|) with |E| the k-NN edge count, capped so
@@ -361,9 +374,6 @@ void mst_over_subset(Graph& g, Scratch& s, const uint32_t* d_sel, uint32_t m, st
     s.sub_pts.ensure(static_cast<uint64_t>(m) * g.stride * 4);
     s.sub_core.ensure(m * 4ull);
     s.mat.ensure(static_cast<uint64_t>(m) * m * 4);
-    s.pbest.ensure(m * 4ull);
-    s.pfrom.ensure(m * 4ull);
-    s.pintree.ensure(m + 16ull);
     s.pout.ensure(m * sizeof(cs_edge) + 64);
     s.pcnt.ensure(64);
     k_gather<<<m, 128, 0, c.stream>>>(g.pts.as<float>(), g.stride, g.dists.as<float>(), g.counts.as<uint32_t>(), g.k, d_sel,
@@ -371,9 +381,10 @@ void mst_over_subset(Graph& g, Scratch& s, const uint32_t* d_sel, uint32_t m, st
     const uint64_t cells = static_cast<uint64_t>(m) * m;
     k_mrd<<<blocks_for(cells), kThreads, 0, c.stream>>>(s.sub_pts.as<float>(), m, g.stride, g.metric, s.sub_core.as<float>(),
                                                        0, m, s.mat.as<float>());
-    k_prim<<<1, 1024, 0, c.stream>>>(s.mat.as<float>(), m, s.sub_pts.as<float>(), g.stride, g.metric, d_sel,
-                                     s.pbest.as<float>(), s.pfrom.as<uint32_t>(), s.pintree.as<uint8_t>(),
-                                     s.pout.as<cs_edge>(), s.pcnt.as<uint32_t>());
+    const size_t prim_smem = static_cast<size_t>(m) * 9;  // best, from, in-tree
+    CSB_CUDA(cudaFuncSetAttribute(k_prim, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(prim_smem)));
+    k_prim<<<1, 1024, prim_smem, c.stream>>>(s.mat.as<float>(), m, s.sub_pts.as<float>(), g.stride, g.metric, d_sel,
+                                             s.pout.as<cs_edge>(), s.pcnt.as<uint32_t>());
     count_launch(c, 3);
     check_launch(c, "bridge MST");
     uint32_t cnt = 0;
@@ -437,9 +448,6 @@ void bridges_reserve(Graph& g) {
     s.sub_pts.ensure(md * g.stride * 4);
     s.sub_core.ensure(md * 4);
     s.mat.ensure(md * md * 4);
-    s.pbest.ensure(md * 4);
-    s.pfrom.ensure(md * 4);
-    s.pintree.ensure(md + 16);
     s.pout.ensure(md * sizeof(cs_edge) + 64);
     s.pcnt.ensure(64);
     g.ctx->scratch[6].ensure(m * 16 + 16);
