@@ -131,12 +131,28 @@ __global__ void k_collect(const unsigned long long* __restrict__ ks, const unsig
 }
 
 /// One quota round: per component, the lowest (score) then lowest (rdeg, id) among
-/// the nodes not yet taken by an earlier quota round.
+/// the nodes not yet taken by an earlier quota round.  A warp whose candidate nodes
+/// all lie in one component (the usual case: a k-NN graph has few components, and
+/// one atomic per node on its key serialised) offers their minimum once.
 __global__ void k_quota_score(const unsigned long long* __restrict__ ks, const uint32_t* __restrict__ comp, uint32_t n,
                               const uint8_t* __restrict__ qtaken, unsigned long long* __restrict__ best_s) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n || qtaken[v]) return;
-    atomicMin(best_s + comp[v], ks[v]);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;  // every lane reaches the warp votes
+    const unsigned lane = threadIdx.x & 31u;
+    const bool ok = v < n && !qtaken[v];
+    const uint32_t c = ok ? comp[v] : 0u;
+    unsigned long long x = ok ? ks[v] : kNoKey;
+    const unsigned live = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!live) return;
+    const uint32_t c0 = __shfl_sync(0xFFFFFFFFu, c, __ffs(live) - 1);
+    if (__all_sync(0xFFFFFFFFu, !ok || c == c0)) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long y = __shfl_xor_sync(0xFFFFFFFFu, x, o);
+            x = y < x ? y : x;
+        }
+        if (lane == 0) atomicMin(best_s + c0, x);
+    } else if (ok) {
+        atomicMin(best_s + c, x);
+    }
 }
 __global__ void k_quota_tie(const unsigned long long* __restrict__ ks, const unsigned long long* __restrict__ kt,
                             const uint32_t* __restrict__ comp, uint32_t n, const uint8_t* __restrict__ qtaken,
