@@ -21,8 +21,8 @@ def test_mixture_is_reproducible():
 
 
 def test_mixture_noise_share_and_box():
-    """The noise rows are uniform over the clustered rows' bounding box, so the whole
-    set's box is the clustered one; without noise every row is near a centre."""
+    """Without noise every row lies near a centre; with 20 % noise (uniform over the
+    clustered rows' bounding box) about that share lies far from every centre."""
     centres = np.random.default_rng(9).uniform(0.0, 10.0, size=(5, 8))
     x = datagen.gaussian_mixture(3000, 8, 5, sigma=(0.1, 0.1), noise=0.0, seed=9, centres=centres)
     d = np.min(np.linalg.norm(x[:, None, :].astype(np.float64) - centres[None], axis=2), axis=1)
