@@ -415,10 +415,16 @@ void cs_host_free(void* p);
  * optional); the scalars go to host memory (optional).  All scratch lives in one
  * fixed 12 MiB __device__ array of this library, held by every GPU that loads the
  * library until the process exits; limits: n <= 131072 nodes, m <= 1048576 edges,
- * larger sizes are rejected with CS_ERR_INVALID.  Runs on the current device and
- * `stream` (a cudaStream_t; NULL is the default stream); needs no cs_ctx; errors
- * via cs_last_error(NULL).  The first call on a device looks up the array's
- * address (cudaGetSymbolAddress) and should come before any stream capture.  Every
+ * larger sizes are rejected with CS_ERR_INVALID.  Edges must have both endpoints
+ * below n and weights that are non-negative with the sign bit clear and not NaN
+ * (+inf is allowed); a list that breaks this is rejected with CS_ERR_INVALID before
+ * any Boruvka round runs.  Runs on the current device, in the current CUDA context,
+ * and on `stream` (a cudaStream_t; NULL is the default stream); needs no cs_ctx;
+ * errors via cs_last_error(NULL).  The array's device address belongs to the
+ * current context, so every call looks it up (cudaGetSymbolAddress) with the
+ * caller's device and context current.  The call synchronises `stream` (the host
+ * reads a counter after every Boruvka round) and returns with the results written:
+ * it blocks the host and must not be called while `stream` is capturing.  Every
  * call reuses the same array (its contents are re-initialised per call), so calls
  * that overlap on the GPU -- from two streams or two host threads on one device --
  * race: serialise them.  Same result as cs_extract on the same edges: the unique

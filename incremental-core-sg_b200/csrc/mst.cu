@@ -584,27 +584,40 @@ constexpr size_t kNoAllocScratchBytes = size_t(12) << 20;  // 12 MiB per GPU
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-constexpr int kNoAllocMaxDevices = 64;
-unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
-
-/// Device address of the scratch array on the current device.  The first call on
-/// a device looks it up with cudaGetSymbolAddress (with that device current) and
-/// caches it; later calls only read the cache.
-unsigned char* noalloc_scratch(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices) fail(CS_ERR_UNSUPPORTED, "cs_mst_noalloc: device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) {
-            cudaGetLastError();
-            fail(CS_ERR_CUDA, std::string("cs_mst_noalloc: cudaGetSymbolAddress of the scratch array failed: ") +
-                                  cudaGetErrorString(e));
-        }
-        g_noalloc_addr[device] = static_cast<unsigned char*>(ptr);
+/// Device address of the scratch array in the current context.  An address of a
+/// __device__ variable belongs to one CUDA context (a caller that makes its own
+/// context current, or resets the device, gets a different one), so it is looked up
+/// on every call, with the caller's device current, and never cached.
+unsigned char* noalloc_scratch() {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        fail(CS_ERR_CUDA, std::string("cs_mst_noalloc: cudaGetSymbolAddress of the scratch array failed: ") +
+                              cudaGetErrorString(e));
     }
-    return g_noalloc_addr[device];
+    return static_cast<unsigned char*>(ptr);
+}
+
+constexpr int kNoAllocBadEndpoint = 1;
+constexpr int kNoAllocBadWeight = 2;
+
+/// Input check of a caller's edge list: every endpoint below n, every weight
+/// non-negative with the sign bit clear and not NaN (+inf is allowed: an empty
+/// neighbourhood has an infinite core distance).  The packed (weight bits, index) key
+/// orders weights only under those conditions, and the Boruvka kernels index node
+/// arrays by the endpoints without range checks.
+__global__ void k_noalloc_check(const uint32_t* __restrict__ eu, const uint32_t* __restrict__ ev,
+                                const float* __restrict__ ew, uint64_t m, uint32_t n, int* bad) {
+    int flags = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < m;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (eu[i] >= n || ev[i] >= n) flags |= kNoAllocBadEndpoint;
+        const uint32_t b = __float_as_uint(ew[i]);
+        if ((b >> 31) || (b & 0x7FFFFFFFu) > 0x7F800000u) flags |= kNoAllocBadWeight;
+    }
+    flags = __reduce_or_sync(0xFFFFFFFFu, flags);
+    if (flags && (threadIdx.x & 31u) == 0) atomicOr(bad, flags);
 }
 
 struct Carver {
@@ -657,7 +670,7 @@ extern "C" cs_status cs_mst_noalloc(const uint32_t* d_u, const uint32_t* d_v, co
         }
         int device = 0;
         CSB_CUDA(cudaGetDevice(&device));
-        Carver cv{noalloc_scratch(device)};
+        Carver cv{noalloc_scratch()};
         const cudaStream_t s = static_cast<cudaStream_t>(stream);
         // a stack Ctx only carries the stream to the shared launch helpers; it owns
         // no device memory
@@ -688,10 +701,22 @@ extern "C" cs_status cs_mst_noalloc(const uint32_t* d_u, const uint32_t* d_v, co
         CSB_CUDA(cudaMemsetAsync(mv.ctr, 0, 64, s));
         CSB_CUDA(cudaMemsetAsync(status, 0, 64, s));
         CSB_CUDA(cudaMemsetAsync(counts, 0, 64, s));
-        k_iota<<<blocks_for(n), kThreads, 0, s>>>(mv.parent, n, n);
         int sms = 148;
         CSB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
         const unsigned grid_cap = static_cast<unsigned>(sms) * 8u;
+        if (m > 0) {
+            int bad = 0;
+            k_noalloc_check<<<std::min<unsigned>(grid_cap, blocks_for(m)), kThreads, 0, s>>>(d_u, d_v, d_w, m, n,
+                                                                                           status + 1);
+            CSB_CUDA(cudaGetLastError());
+            CSB_CUDA(cudaMemcpyAsync(&bad, status + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CSB_CUDA(cudaStreamSynchronize(s));
+            if (bad & kNoAllocBadEndpoint)
+                fail(CS_ERR_INVALID, "cs_mst_noalloc: an edge endpoint is >= n = " + std::to_string(n));
+            if (bad & kNoAllocBadWeight)
+                fail(CS_ERR_INVALID, "cs_mst_noalloc: an edge weight is negative (sign bit set) or NaN");
+        }
+        k_iota<<<blocks_for(n), kThreads, 0, s>>>(mv.parent, n, n);
         uint32_t in_count = static_cast<uint32_t>(m);
         uint32_t hc[4];
         int r = 0;
