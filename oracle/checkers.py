@@ -199,6 +199,13 @@ class Reference:
         _sig(lib, "ref_last_error", C.c_char_p)
         _sig(lib, "ref_metric_distance", _f32, _p, _p, _u32)
         _sig(lib, "ref_build", _p, _p, _u64, _u32, _u32, _u32, _u32, _u32, _u64, _u32, _p)
+        _sig(lib, "ref_build_m", _p, _p, _u64, _u32, _u32, _u32, _u32, _u32, _u64, _u32, C.c_int, _p)
+        _sig(lib, "ref_metric_distance_m", _f32, C.c_int, _p, _p, _u32)
+        _sig(lib, "ref_dataset_rows", None, _p, _u64, _u32, C.c_int, _p)
+        _sig(lib, "ref_from_state_m", _p, _p, _u64, _u32, _u32, _u32, _p, _p, _p, _p, _p, _u64, _u64, _u32,
+             C.c_int)
+        _sig(lib, "ref_nndescent_m", C.c_int, _p, _u64, _u32, _u32, _u32, _u32, _f64, _u64, _u32, C.c_int,
+             _p, _p, _p, _p, _p)
         _sig(lib, "ref_insert", C.c_int, _p, _p, _u64, _p)
         _sig(lib, "ref_from_state", _p, _p, _u64, _u32, _u32, _u32, _p, _p, _p, _p, _p, _u64, _u64, _u32)
         _sig(lib, "ref_free", None, _p)
@@ -240,27 +247,37 @@ class Reference:
         if self.lib.ref_write_labels_tsv(str(path).encode(), _ptr(lab), len(lab)):
             raise RuntimeError(self.err())
 
-    def metric_distance(self, a, b):
+    def metric_distance(self, a, b, metric=0):
+        """metric_distance (include/coresg/distance.hpp) under metric code `metric`
+        (0 L2, 1 cosine on normalised rows)."""
         a = np.ascontiguousarray(a, np.float32)
         b = np.ascontiguousarray(b, np.float32)
-        return np.float32(self.lib.ref_metric_distance(_ptr(a), _ptr(b), a.shape[-1]))
+        return np.float32(self.lib.ref_metric_distance_m(metric, _ptr(a), _ptr(b), a.shape[-1]))
 
-    def build(self, rows, k_max=32, instances=1, iters=10, sample=16, seed=42, threads=0):
+    def dataset_rows(self, rows, metric=0):
+        """The padded rows Dataset::append stores (cosine rows normalised)."""
+        rows = np.ascontiguousarray(rows, np.float32)
+        n, d = rows.shape
+        out = np.empty((n, (d + 7) & ~7), np.float32)
+        self.lib.ref_dataset_rows(_ptr(rows), n, d, metric, _ptr(out))
+        return out
+
+    def build(self, rows, k_max=32, instances=1, iters=10, sample=16, seed=42, threads=0, metric=0):
         rows = np.ascontiguousarray(rows, np.float32)
         times = np.zeros(4, np.float64)
-        h = self.lib.ref_build(_ptr(rows), rows.shape[0], rows.shape[1], k_max, instances, iters,
-                               sample, seed, threads, _ptr(times))
+        h = self.lib.ref_build_m(_ptr(rows), rows.shape[0], rows.shape[1], k_max, instances, iters,
+                                 sample, seed, threads, metric, _ptr(times))
         if not h:
             raise RuntimeError(self.err())
         return RefCoreSG(self, h, times)
 
-    def from_state(self, padded, dim, ids, dists, flags, counts, bridges, repair=0, threads=0):
+    def from_state(self, padded, dim, ids, dists, flags, counts, bridges, repair=0, threads=0, metric=0):
         n, stride = padded.shape
         k = ids.shape[1]
         bridges = np.ascontiguousarray(bridges, EDGE_DTYPE)
-        h = self.lib.ref_from_state(_ptr(padded), n, dim, stride, k, _ptr(ids), _ptr(dists),
-                                    _ptr(flags), _ptr(counts), _ptr(bridges), len(bridges), repair,
-                                    threads)
+        h = self.lib.ref_from_state_m(_ptr(padded), n, dim, stride, k, _ptr(ids), _ptr(dists),
+                                      _ptr(flags), _ptr(counts), _ptr(bridges), len(bridges), repair,
+                                      threads, metric)
         if not h:
             raise RuntimeError(self.err())
         return RefCoreSG(self, h, np.zeros(4))
@@ -283,16 +300,16 @@ class Reference:
                                                  _ptr(dists), _ptr(counts), k, queries, seed,
                                                  threads or os.cpu_count()))
 
-    def nndescent(self, rows, k=32, sample=16, iters=10, delta=0.001, seed=42, threads=0):
+    def nndescent(self, rows, k=32, sample=16, iters=10, delta=0.001, seed=42, threads=0, metric=0):
         rows = np.ascontiguousarray(rows, np.float32)
         n = rows.shape[0]
         ids = np.empty((n, k), np.uint32)
         dists = np.empty((n, k), np.float32)
         counts = np.empty(n, np.uint32)
         ev, sec = _u64(), _f64()
-        rc = self.lib.ref_nndescent(_ptr(rows), n, rows.shape[1], k, sample, iters, delta, seed,
-                                    threads or os.cpu_count(), _ptr(ids), _ptr(dists), _ptr(counts),
-                                    C.byref(ev), C.byref(sec))
+        rc = self.lib.ref_nndescent_m(_ptr(rows), n, rows.shape[1], k, sample, iters, delta, seed,
+                                      threads or os.cpu_count(), metric, _ptr(ids), _ptr(dists),
+                                      _ptr(counts), C.byref(ev), C.byref(sec))
         if rc:
             raise RuntimeError(self.err())
         return ids, dists, counts, int(ev.value), float(sec.value)

@@ -9,3 +9,9 @@
 extern "C" float refd_metric_distance_l2(const float* a, const float* b, std::uint32_t stride) {
     return coresg::metric_distance(coresg::MetricKind::L2, a, b, stride);
 }
+
+/// metric_distance for any of the reference's metrics (0 L2, 1 cosine on normalised
+/// rows, 2 L1, 3 inner product), with the reference's flags.
+extern "C" float refd_metric_distance(int metric, const float* a, const float* b, std::uint32_t stride) {
+    return coresg::metric_distance(static_cast<coresg::MetricKind>(metric), a, b, stride);
+}

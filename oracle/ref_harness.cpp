@@ -29,6 +29,7 @@
 using namespace coresg;
 
 extern "C" float refd_metric_distance_l2(const float* a, const float* b, std::uint32_t stride);
+extern "C" float refd_metric_distance(int metric, const float* a, const float* b, std::uint32_t stride);
 
 namespace {
 
@@ -40,10 +41,11 @@ struct Handle {
 };
 
 CoreSGParams make_params(std::uint32_t k_max, std::uint32_t instances, std::uint32_t iters,
-                         std::uint32_t sample, std::uint64_t seed, unsigned threads) {
+                         std::uint32_t sample, std::uint64_t seed, unsigned threads, int metric = 0) {
     // Mirrors coresg_cli build (apps/coresg_cli.cpp:81-177) with --gpu 0.
     CoreSGParams p;
     p.k_max = k_max;
+    p.metric = static_cast<MetricKind>(metric);
     p.threads = threads;
     p.seed = seed;
     p.backend.prefer_gpu = false;
@@ -83,13 +85,27 @@ float ref_metric_distance(const float* a, const float* b, std::uint32_t stride) 
     return refd_metric_distance_l2(a, b, stride);
 }
 
-/// CoreSG::build over `n` rows of `dim` floats (reference path, CPU backend).
-void* ref_build(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k_max,
-                std::uint32_t instances, std::uint32_t iters, std::uint32_t sample,
-                std::uint64_t seed, std::uint32_t threads, double* times4) {
+/// metric_distance under metric code `metric` (MetricKind order: 0 L2, 1 cosine).
+float ref_metric_distance_m(int metric, const float* a, const float* b, std::uint32_t stride) {
+    return refd_metric_distance(metric, a, b, stride);
+}
+
+/// The padded rows Dataset::append stores for `n` rows of `dim` floats under
+/// `metric` (cosine rows are L2-normalised, dataset.hpp normalise).
+void ref_dataset_rows(const float* rows, std::uint64_t n, std::uint32_t dim, int metric, float* out_padded) {
+    Dataset data(dim, static_cast<MetricKind>(metric));
+    data.append(rows, static_cast<std::size_t>(n));
+    std::memcpy(out_padded, data.data(), n * data.stride() * sizeof(float));
+}
+
+/// CoreSG::build over `n` rows of `dim` floats (reference path, CPU backend) under
+/// metric code `metric`.
+void* ref_build_m(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k_max,
+                  std::uint32_t instances, std::uint32_t iters, std::uint32_t sample,
+                  std::uint64_t seed, std::uint32_t threads, int metric, double* times4) {
     try {
         auto h = std::make_unique<Handle>();
-        h->sg = std::make_unique<CoreSG>(make_params(k_max, instances, iters, sample, seed, threads));
+        h->sg = std::make_unique<CoreSG>(make_params(k_max, instances, iters, sample, seed, threads, metric));
         h->stats = h->sg->build(rows, static_cast<std::size_t>(n), dim);
         if (times4) {
             times4[0] = h->stats.knn_seconds;
@@ -102,6 +118,13 @@ void* ref_build(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint
         g_err = e.what();
         return nullptr;
     }
+}
+
+/// CoreSG::build under L2.
+void* ref_build(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k_max,
+                std::uint32_t instances, std::uint32_t iters, std::uint32_t sample,
+                std::uint64_t seed, std::uint32_t threads, double* times4) {
+    return ref_build_m(rows, n, dim, k_max, instances, iters, sample, seed, threads, 0, times4);
 }
 
 /// CoreSG::insert of `count` further rows.
@@ -119,11 +142,11 @@ int ref_insert(void* hp, const float* rows, std::uint64_t count, double* total_s
 
 /// Adopt a given state (padded points, k-NN arrays, bridges) through CoreSG::load,
 /// which re-derives connectivity and hubness exactly as `coresg_cli extract` does.
-void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
-                     std::uint32_t stride, std::uint32_t k_max, const std::uint32_t* ids,
-                     const float* dists, const std::uint8_t* flags, const std::uint32_t* counts,
-                     const void* bridges, std::uint64_t n_bridges, std::uint64_t repair,
-                     std::uint32_t threads) {
+void* ref_from_state_m(const float* padded, std::uint64_t n, std::uint32_t dim,
+                       std::uint32_t stride, std::uint32_t k_max, const std::uint32_t* ids,
+                       const float* dists, const std::uint8_t* flags, const std::uint32_t* counts,
+                       const void* bridges, std::uint64_t n_bridges, std::uint64_t repair,
+                       std::uint32_t threads, int metric) {
     char path[] = "/tmp/coresg_ref_XXXXXX";
     const int fd = mkstemp(path);
     if (fd < 0) {
@@ -139,7 +162,7 @@ void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
             put(os, k_max);
             put(os, dim);
             put(os, stride);
-            put(os, std::uint32_t(0));  // metric L2
+            put(os, std::uint32_t(metric));
             put(os, std::uint32_t(0));  // missing mode AntiHub
             put(os, std::uint64_t(n));
             put_vec(os, padded, n * stride);
@@ -151,7 +174,7 @@ void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
             put(os, std::uint64_t(repair));
         }
         auto h = std::make_unique<Handle>();
-        h->sg = std::make_unique<CoreSG>(make_params(k_max, 1, 10, 16, 42, threads));
+        h->sg = std::make_unique<CoreSG>(make_params(k_max, 1, 10, 16, 42, threads, metric));
         h->sg->load(path);
         std::remove(path);
         return h.release();
@@ -160,6 +183,16 @@ void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
         g_err = e.what();
         return nullptr;
     }
+}
+
+/// ref_from_state_m under L2.
+void* ref_from_state(const float* padded, std::uint64_t n, std::uint32_t dim,
+                     std::uint32_t stride, std::uint32_t k_max, const std::uint32_t* ids,
+                     const float* dists, const std::uint8_t* flags, const std::uint32_t* counts,
+                     const void* bridges, std::uint64_t n_bridges, std::uint64_t repair,
+                     std::uint32_t threads) {
+    return ref_from_state_m(padded, n, dim, stride, k_max, ids, dists, flags, counts, bridges, n_bridges, repair,
+                            threads, 0);
 }
 
 void ref_free(void* hp) { delete static_cast<Handle*>(hp); }
@@ -366,12 +399,12 @@ double ref_sampled_recall(const float* rows, std::uint64_t n, std::uint32_t dim,
 
 /// The reference's CPU NN-Descent alone (init_random + nndescent), as the CPU
 /// backend runs one k-NN job (src/cpu_backend.cpp:47-59).
-int ref_nndescent(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k,
-                  std::uint32_t sample, std::uint32_t iters, double delta, std::uint64_t seed,
-                  std::uint32_t threads, std::uint32_t* ids, float* dists,
-                  std::uint32_t* counts, std::uint64_t* evals, double* seconds) {
+int ref_nndescent_m(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k,
+                    std::uint32_t sample, std::uint32_t iters, double delta, std::uint64_t seed,
+                    std::uint32_t threads, int metric, std::uint32_t* ids, float* dists,
+                    std::uint32_t* counts, std::uint64_t* evals, double* seconds) {
     try {
-        Dataset data(dim, MetricKind::L2);
+        Dataset data(dim, static_cast<MetricKind>(metric));
         data.append(rows, static_cast<std::size_t>(n));
         KnnGraph g(static_cast<idx_t>(n), k);
         ThreadPool pool(threads ? threads : 1);
@@ -394,6 +427,15 @@ int ref_nndescent(const float* rows, std::uint64_t n, std::uint32_t dim, std::ui
         g_err = e.what();
         return 1;
     }
+}
+
+/// ref_nndescent_m under L2.
+int ref_nndescent(const float* rows, std::uint64_t n, std::uint32_t dim, std::uint32_t k,
+                  std::uint32_t sample, std::uint32_t iters, double delta, std::uint64_t seed,
+                  std::uint32_t threads, std::uint32_t* ids, float* dists,
+                  std::uint32_t* counts, std::uint64_t* evals, double* seconds) {
+    return ref_nndescent_m(rows, n, dim, k, sample, iters, delta, seed, threads, 0, ids, dists, counts, evals,
+                           seconds);
 }
 
 }  // extern "C"
