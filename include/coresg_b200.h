@@ -87,6 +87,11 @@ void cs_ctx_destroy(cs_ctx* ctx);
 /* Release cached scratch (coresg::cuda::release_thread_cache, cuda_api.hpp:84;
  * Backend::trim, backend.hpp:91). */
 cs_status cs_ctx_trim(cs_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), on which every call of this context
+ * runs its device work: a caller orders its own work after the engine's on it (the
+ * multi-GPU gather of a partitioned sweep runs its collective there).  Valid until
+ * cs_ctx_destroy. */
+void* cs_ctx_stream(const cs_ctx* ctx);
 /* Number of engine kernel launches issued on this context so far. */
 uint64_t cs_ctx_launches(const cs_ctx* ctx);
 /* Device allocations (cudaMalloc) the library has made in this process so far,
@@ -242,6 +247,23 @@ cs_status cs_insert(cs_graph* g, const float* rows, uint64_t count, uint32_t row
  * CoreSGParams/HubnessParams.  Results: the graph's bridge set; counts optional. */
 cs_status cs_select_bridges(cs_graph* g, uint64_t* out_selected, uint64_t* out_bridges,
                             uint64_t* out_repair, uint32_t* out_knn_components);
+/* Stages of the last cs_select_bridges (or of the re-selection inside cs_insert),
+ * device milliseconds between stage boundaries on the context stream (host steps
+ * between them included), as CoreSGStats::hubness_seconds / missing_seconds /
+ * repair_seconds (include/coresg/coresg.hpp:108-138) and HubnessStats
+ * (include/coresg/hubness.hpp:121-142) split the reference's build. */
+typedef struct {
+    double connectivity_ms;  /* union-find over the k-NN lists, dense component labels */
+    double hubness_ms;       /* reverse degrees and scores */
+    double edges_ms;         /* the undirected k-NN edge list (its count is the budget's |E|) */
+    double selection_ms;     /* budget-lowest selection, per-component quota, ordering */
+    double bridge_mst_ms;    /* dense MRD + Prim over the selected anti-hubs */
+    double repair_ms;        /* connectivity repair (0 when the bridges join every component) */
+    double total_ms;
+    uint64_t selected, bridges, repair;
+    uint32_t knn_components, reserved0;
+} cs_bridge_stats;
+cs_status cs_bridge_stats_get(cs_graph* g, cs_bridge_stats* out);
 /* The selected anti-hubs of the last cs_select_bridges (HubnessIndex::selected). */
 cs_status cs_get_selected(cs_graph* g, uint32_t* out, uint64_t cap, uint64_t* out_count);
 
@@ -287,6 +309,13 @@ cs_status cs_extract_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, cs_edg
 cs_status cs_extract_sweep_device(cs_graph* g, const uint32_t* mpts, uint32_t K, float* out_ms);
 cs_status cs_sweep_fetch(cs_graph* g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels,
                          uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
+/* cs_sweep_fetch into caller DEVICE buffers on the graph's device (the tree:
+ * nedges entries of d_out_edges; the labels: n entries of d_out_labels; either may be
+ * NULL), copied device to device on the context stream, complete on return; the
+ * scalars go to host memory.  For handing results to a collective (the multi-GPU
+ * gather of a partitioned sweep) without a host round trip. */
+cs_status cs_sweep_fetch_device(cs_graph* g, uint32_t index, cs_edge* d_out_edges, uint32_t* d_out_labels,
+                                uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight);
 
 /* Device times of the last sweep: the whole captured sequence and the persistent
  * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
@@ -404,6 +433,22 @@ cs_status cs_server_stats_get(cs_server* s, cs_server_stats* out);
  * asynchronously only into pinned memory). */
 void* cs_host_alloc(size_t bytes);
 void cs_host_free(void* p);
+
+/* ---- testing hooks (no counterpart in the reference) --------------------------
+ * Failure paths made on purpose, without a GPU fault: a bounded wait that runs out
+ * and a device allocation that fails.  Not for production use. */
+
+/* Grid-barrier wait limit of later sweeps on g in nanoseconds (0: the default, 2 s),
+ * and a delay block 0 of the persistent sweep kernel takes (a bounded sleep) before
+ * its first grid barrier (0: none; at most 5 s).  With hold_ns above limit_ns the
+ * other blocks' waits run out: the sweep returns CS_ERR_TIMEOUT, its results are not
+ * valid, and the context and graph stay usable.  Plans are recaptured when these
+ * change. */
+cs_status cs_test_sweep_barrier(cs_graph* g, uint64_t limit_ns, uint64_t hold_ns);
+/* Process-wide: after `after` further device allocations by the library succeed,
+ * every later one fails with CS_ERR_OOM (no cudaMalloc is issued for it);
+ * UINT64_MAX switches the injection off. */
+void cs_test_fail_device_allocs(uint64_t after);
 
 /* ---- allocation-free MST (no counterpart in the reference) ------------------- */
 

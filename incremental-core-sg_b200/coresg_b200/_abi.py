@@ -72,17 +72,22 @@ _SIGS = {
     "cs_insert": (_i32, [_p, _p, _u64, _u32, _p, _p, _p]),
     "cs_insert_stats_get": (_i32, [_p, _p]),
     "cs_get_selected": (_i32, [_p, _p, _u64, _p]),
+    "cs_bridge_stats_get": (_i32, [_p, _p]),
     "cs_core_distances": (_i32, [_p, _u32, _p]),
     "cs_edges": (_i32, [_p, _u32, _p, _u64, _p]),
     "cs_extract": (_i32, [_p, _u32, _p, _p, _p, _p, _p]),
     "cs_extract_sweep": (_i32, [_p, _p, _u32, _p, _p, _p, _p, _p]),
     "cs_extract_sweep_device": (_i32, [_p, _p, _u32, _p]),
     "cs_sweep_fetch": (_i32, [_p, _u32, _p, _p, _p, _p, _p]),
+    "cs_sweep_fetch_device": (_i32, [_p, _u32, _p, _p, _p, _p, _p]),
     "cs_sweep_timing": (_i32, [_p, _p, _p]),
     "cs_sweep_trace": (_i32, [_p, _p, _u32, _p]),
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
+    "cs_ctx_stream": (_p, [_p]),
     "cs_mst_noalloc": (_i32, [_p, _p, _p, _u64, _u32, _p, _p, _p, _p, _p, _p]),
+    "cs_test_sweep_barrier": (_i32, [_p, _u64, _u64]),
+    "cs_test_fail_device_allocs": (None, [_u64]),
     "cs_server_create": (_i32, [_p, _p, _pp]),
     "cs_server_destroy": (None, [_p]),
     "cs_server_submit": (_i32, [_p, _p, _p]),
@@ -142,6 +147,19 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def device_props(device: int = 0) -> dict:
+    """cs_device_props: name, memory, SM count and compute capability of a device."""
+    name = C.create_string_buffer(256)
+    total, free = C.c_size_t(), C.c_size_t()
+    sms, major, minor = C.c_int32(), C.c_int32(), C.c_int32()
+    st = lib().cs_device_props(device, name, 256, C.byref(total), C.byref(free), C.byref(sms), C.byref(major),
+                               C.byref(minor))
+    if st != CS_OK:
+        raise CsError(st, lib().cs_last_error(None).decode())
+    return dict(name=name.value.decode(), total_mem=total.value, free_mem=free.value, sm_count=sms.value,
+                cc=(major.value, minor.value))
+
+
 def device_count() -> int:
     n = C.c_int32(0)
     lib().cs_device_count(C.byref(n))
@@ -161,6 +179,11 @@ class Context:
     def check(self, st):
         if st != CS_OK:
             raise CsError(st, lib().cs_last_error(self.h).decode())
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t (cs_ctx_stream) as an integer handle."""
+        return int(lib().cs_ctx_stream(self.h) or 0)
 
     @property
     def launches(self) -> int:
@@ -217,6 +240,13 @@ class InsertStats(C.Structure):
                 ("reverse_ms", C.c_double), ("search_ms", C.c_double), ("instance_ms", C.c_double),
                 ("refine_ms", C.c_double), ("finish_ms", C.c_double), ("bridges_ms", C.c_double),
                 ("total_ms", C.c_double)]
+
+
+class BridgeStats(C.Structure):
+    _fields_ = [("connectivity_ms", C.c_double), ("hubness_ms", C.c_double), ("edges_ms", C.c_double),
+                ("selection_ms", C.c_double), ("bridge_mst_ms", C.c_double), ("repair_ms", C.c_double),
+                ("total_ms", C.c_double), ("selected", C.c_uint64), ("bridges", C.c_uint64), ("repair", C.c_uint64),
+                ("knn_components", C.c_uint32), ("reserved0", C.c_uint32)]
 
 
 class MstResult:
@@ -345,6 +375,12 @@ class CoreSG:
         self.ctx.check(lib().cs_select_bridges(self.h, C.byref(sel), C.byref(br), C.byref(rep), C.byref(comp)))
         return dict(selected=sel.value, bridges=br.value, repair=rep.value, knn_components=comp.value)
 
+    def bridge_stats(self) -> dict:
+        """Stages of the last bridge selection (cs_bridge_stats_get)."""
+        x = BridgeStats()
+        self.ctx.check(lib().cs_bridge_stats_get(self.h, C.byref(x)))
+        return {name: getattr(x, name) for name, _ in BridgeStats._fields_ if name != "reserved0"}
+
     def selected(self):
         cnt = C.c_uint64(0)
         self.ctx.check(lib().cs_get_selected(self.h, None, 0, C.byref(cnt)))
@@ -437,6 +473,15 @@ class CoreSG:
         self.ctx.check(lib().cs_sweep_fetch(self.h, index, _ptr(edges), _ptr(lab), C.byref(ne), C.byref(nc),
                                             C.byref(w)))
         return MstResult(edges[:ne.value], None if lab is None else lab[:n], nc.value, w.value)
+
+    def sweep_fetch_device(self, index: int, d_edges: int, d_labels: int | None) -> dict:
+        """Result `index` of the last sweep into device buffers (raw device addresses
+        on this graph's device, e.g. torch tensors' data_ptr()); returns the scalars."""
+        ne, nc, w = C.c_uint64(), C.c_uint32(), C.c_double()
+        self.ctx.check(lib().cs_sweep_fetch_device(self.h, index, C.c_void_p(d_edges),
+                                                   C.c_void_p(d_labels) if d_labels else None, C.byref(ne),
+                                                   C.byref(nc), C.byref(w)))
+        return dict(nedges=ne.value, ncomp=nc.value, weight=w.value)
 
     def sweep_trace(self) -> np.ndarray:
         """Per-round profile of the last sweep's first pass: columns phase A ns,

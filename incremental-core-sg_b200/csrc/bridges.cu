@@ -470,6 +470,33 @@ void bridges_reserve(Graph& g) {
     g.bridges.grow_keep(md * sizeof(cs_edge), g.ctx->stream);
 }
 
+/// Events recorded on a stream at stage boundaries; elapsed() gives the
+/// milliseconds between consecutive marks once the last one has completed.
+struct StageEvents {
+    static constexpr int kMax = 12;
+    cudaStream_t s;
+    cudaEvent_t ev[kMax] = {};
+    int n = 0;
+    explicit StageEvents(cudaStream_t st) : s(st) {}
+    ~StageEvents() {
+        for (int i = 0; i < n; ++i) cudaEventDestroy(ev[i]);
+    }
+    void mark() {
+        if (n == kMax) return;
+        CSB_CUDA(cudaEventCreate(&ev[n]));
+        CSB_CUDA(cudaEventRecord(ev[n], s));
+        ++n;
+    }
+    void elapsed(double* out, int count) {
+        if (n) CSB_CUDA(cudaEventSynchronize(ev[n - 1]));
+        for (int i = 0; i < count; ++i) {
+            float t = 0.0f;
+            if (i + 1 < n) CSB_CUDA(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+            out[i] = t;
+        }
+    }
+};
+
 void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uint64_t* out_repair,
                     uint32_t* out_components) {
     Ctx& c = *g.ctx;
@@ -477,6 +504,8 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     const uint32_t k = g.k;
     CSB_REQUIRE(n > 0, "cs_select_bridges: empty graph");
     Scratch s(g);
+    StageEvents ev(c.stream);
+    ev.mark();
     int* status = c.status.as<int>();
     CSB_CUDA(cudaMemsetAsync(status, 0, 4, c.stream));
     const uint64_t nk = static_cast<uint64_t>(n) * k;
@@ -493,6 +522,7 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     count_launch(c, 2);
     launch_labels(c, s.parent.as<uint32_t>(), n, 1, s.lab.as<uint32_t>(), s.bc.as<uint32_t>(),
                   s.ncomp.as<unsigned long long>());
+    ev.mark();  // connectivity
     // ---- hubness
     s.rdeg.ensure(ns * 4ull);
     s.score.ensure(ns * 8ull);
@@ -505,6 +535,7 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
                                                       s.ks.as<unsigned long long>(), s.kt.as<unsigned long long>());
     count_launch(c, 2);
     check_launch(c, "hubness");
+    ev.mark();  // hubness
     unsigned long long ncomp64 = 0;
     CSB_CUDA(cudaMemcpyAsync(&ncomp64, s.ncomp.p, 8, cudaMemcpyDeviceToHost, c.stream));
     int st = 0;
@@ -515,6 +546,7 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     g.last_ncomp = ncomp;
     // ---- budget
     graph_build_edges(g);
+    ev.mark();  // edge list
     const uint64_t budget = antihub_budget(g.e_knn, g.dim, n);
     // ---- selection: budget lowest under (score, rdeg, id)
     const uint32_t cap = static_cast<uint32_t>(budget + 2ull * ncomp + 8);
@@ -603,9 +635,11 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     }
     g.selected = sel;
     copy_h2d(c, s.sel.p, sel.data(), m * 4ull);
+    ev.mark();  // selection
     // ---- bridge MST over the selected set
     std::vector<cs_edge> missing;
     mst_over_subset(g, s, s.sel.as<uint32_t>(), m, &missing);
+    ev.mark();  // bridge MST
     // ---- repair_connectivity (only a k-NN graph of several components needs it)
     uint64_t added = 0;
     if (ncomp > 1) {
@@ -679,16 +713,33 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
             }
         }
     }
+    ev.mark();  // repair
     // ---- install the bridges
     g.bridges.ensure(std::max<size_t>(missing.size(), 1) * sizeof(cs_edge));
     if (!missing.empty()) copy_h2d(c, g.bridges.p, missing.data(), missing.size() * sizeof(cs_edge));
     g.nb = missing.size();
     g.n_repair = added;
-    g.invalidate_edges();
+    g.invalidate_bridges();
     if (out_selected) *out_selected = m;
     if (out_bridges) *out_bridges = missing.size();
     if (out_repair) *out_repair = added;
     if (out_components) *out_components = ncomp;
+    ev.mark();
+    double ms[7] = {0};
+    ev.elapsed(ms, 7);
+    cs_bridge_stats& bs = g.last_bridges;
+    bs = cs_bridge_stats{};
+    bs.connectivity_ms = ms[0];
+    bs.hubness_ms = ms[1];
+    bs.edges_ms = ms[2];
+    bs.selection_ms = ms[3];
+    bs.bridge_mst_ms = ms[4];
+    bs.repair_ms = ms[5];
+    bs.total_ms = ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5] + ms[6];
+    bs.selected = m;
+    bs.bridges = missing.size();
+    bs.repair = added;
+    bs.knn_components = ncomp;
 }
 
 }  // namespace csb
@@ -722,6 +773,14 @@ cs_status cs_mrd_block(cs_ctx* ctx, const float* host_pts, size_t m, uint32_t di
 cs_status cs_select_bridges(cs_graph* gp, uint64_t* a, uint64_t* b, uint64_t* cc, uint32_t* d) {
     Graph* g = reinterpret_cast<Graph*>(gp);
     return guarded(g ? g->ctx : nullptr, [&] { select_bridges(*g, a, b, cc, d); });
+}
+
+cs_status cs_bridge_stats_get(cs_graph* gp, cs_bridge_stats* out) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(out != nullptr, "cs_bridge_stats_get: null output");
+        *out = g->last_bridges;
+    });
 }
 
 cs_status cs_get_selected(cs_graph* gp, uint32_t* out, uint64_t cap, uint64_t* out_count) {

@@ -17,6 +17,18 @@ void count_alloc(size_t nbytes) {
     g_dev_allocs.fetch_add(1, std::memory_order_relaxed);
     g_dev_alloc_bytes.fetch_add(nbytes, std::memory_order_relaxed);
 }
+// testing hook (cs_test_fail_device_allocs): device allocations still allowed before
+// every further one fails; UINT64_MAX = no injection
+std::atomic<uint64_t> g_fail_after{UINT64_MAX};
+/// True when this allocation must fail by injection (no cudaMalloc is issued).
+bool injected_alloc_failure() {
+    uint64_t v = g_fail_after.load(std::memory_order_relaxed);
+    while (v != UINT64_MAX) {
+        if (v == 0) return true;
+        if (g_fail_after.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return false;
+    }
+    return false;
+}
 }  // namespace
 
 void set_thread_error(const std::string& m) { t_error = m; }
@@ -55,6 +67,8 @@ void DevBuf::ensure(size_t nbytes) {
     if (p) nbytes = std::max(nbytes, bytes + bytes / 4);
     release();
     if (nbytes == 0) nbytes = 16;
+    if (injected_alloc_failure())
+        fail(CS_ERR_OOM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: injected by cs_test_fail_device_allocs");
     void* q = nullptr;
     const cudaError_t e = cudaMalloc(&q, nbytes);
     if (e != cudaSuccess) {
@@ -69,6 +83,8 @@ void DevBuf::ensure(size_t nbytes) {
 
 void DevBuf::grow_keep(size_t nbytes, cudaStream_t s) {
     if (nbytes <= bytes && p) return;
+    if (injected_alloc_failure())
+        fail(CS_ERR_OOM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: injected by cs_test_fail_device_allocs");
     void* q = nullptr;
     const cudaError_t e = cudaMalloc(&q, nbytes);
     if (e != cudaSuccess) {
@@ -317,6 +333,11 @@ cs_status cs_ctx_trim(cs_ctx* ctx) {
     });
 }
 
+void* cs_ctx_stream(const cs_ctx* ctx) {
+    const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
+    return c ? static_cast<void*>(c->stream) : nullptr;
+}
+
 uint64_t cs_ctx_launches(const cs_ctx* ctx) {
     const Ctx* c = reinterpret_cast<const Ctx*>(ctx);
     return c ? c->launches : 0;
@@ -326,5 +347,7 @@ void cs_device_allocs(uint64_t* out_count, uint64_t* out_bytes) {
     if (out_count) *out_count = g_dev_allocs.load(std::memory_order_relaxed);
     if (out_bytes) *out_bytes = g_dev_alloc_bytes.load(std::memory_order_relaxed);
 }
+
+void cs_test_fail_device_allocs(uint64_t after) { g_fail_after.store(after, std::memory_order_relaxed); }
 
 }  // extern "C"

@@ -108,6 +108,7 @@ struct Graph {
     // Derived undirected edge list (base weights), in the reference order:
     // k-NN edges node-major (src/knn_graph.cpp:132-200), then the bridges.
     bool edges_valid = false;
+    bool knn_edges_valid = false;  // the k-NN part (first e_knn entries, node_off) is current
     uint64_t e_knn = 0, e_total = 0;
     DevBuf eu, ev, ew;    // SoA u32/u32/f32 [e_total]
     DevBuf node_off;      // u32 [n+1] offsets of each node's emitted edges
@@ -139,9 +140,17 @@ struct Graph {
     uint32_t sweep_K = 0;                      // MSTs of the last sweep
     uint32_t sweep_block = 0;                  // 0 = autotuned/cached
     uint32_t sweep_flatten = 0xFFFFFFFEu;      // kFlattenAuto, or a divisor (0: never)
+    // testing hook (cs_test_sweep_barrier): grid-barrier wait limit of the sweep
+    // kernel (0: the default) and a delay block 0 takes before its first barrier
+    uint64_t sweep_barrier_ns = 0, sweep_hold_ns = 0;
 
     ~Graph();
-    void invalidate_edges() { edges_valid = false; }
+    void invalidate_edges() { edges_valid = knn_edges_valid = false; }
+    /// Only the bridges changed: the k-NN part of the edge list stays, and the next
+    /// build re-emits the bridge tail alone.
+    void invalidate_bridges() { edges_valid = false; }
+    // Stages of the last cs_select_bridges.
+    cs_bridge_stats last_bridges{};
     void ensure_capacity(uint64_t need, bool keep);
 };
 
@@ -180,7 +189,10 @@ struct MstHost {
 };
 void extract_plain(Graph& g, uint32_t mpts, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
 void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, float* out_ms);
-void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res);
+/// Result `index` of the last sweep: scalars to *res; the tree and labels to host
+/// buffers, or (device_out) to caller device buffers on the graph's device.
+void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res,
+                 bool device_out = false);
 void sweep_free(SweepPlan* p);
 /// Device outputs of MST `index` of the last sweep, valid until the next sweep.
 struct SweepOut {

@@ -244,11 +244,26 @@ void graph_build_edges(Graph& g) {
             if (e.u >= g.n || e.v >= g.n) fail(CS_ERR_STATE, "bridge endpoint out of range for the current graph");
         }
     }
+    // only the bridges changed since the last enumeration: the k-NN edges and their
+    // node offsets stand, and the bridge tail is written after them again
+    if (g.knn_edges_valid && g.eu.bytes / sizeof(uint32_t) >= g.e_knn + g.nb + 1 &&
+        g.e_knn + g.nb <= 0xFFFFFFFEull) {
+        if (g.nb) {
+            k_bridge_emit<<<blocks_for(g.nb), kThreads, 0, c.stream>>>(
+                g.bridges.as<cs_edge>(), g.nb, nullptr, g.eu.as<uint32_t>() + g.e_knn,
+                g.ev.as<uint32_t>() + g.e_knn, g.ew.as<float>() + g.e_knn);
+            count_launch(c);
+            check_launch(c, "bridge edges");
+        }
+        g.e_total = g.e_knn + g.nb;
+        g.edges_valid = true;
+        return;
+    }
     DevBuf core_unused;
     g.e_total = graph_materialize_edges(g, 0, false, g.eu, g.ev, g.ew, core_unused, c.scratch[0],
                                         c.scratch[1], g.node_off);
     g.e_knn = g.e_total - g.nb;
-    g.edges_valid = true;
+    g.edges_valid = g.knn_edges_valid = true;
 }
 
 Graph::~Graph() {
@@ -440,7 +455,7 @@ cs_status cs_graph_set_bridges(cs_graph* gp, const cs_edge* edges, uint64_t m) {
         g->bridges.ensure(std::max<uint64_t>(m, 1) * sizeof(cs_edge));
         copy_h2d(*g->ctx, g->bridges.p, edges, m * sizeof(cs_edge));
         g->nb = m;
-        g->invalidate_edges();
+        g->invalidate_bridges();
     });
 }
 

@@ -91,6 +91,7 @@ struct SweepArgs {
     unsigned* bar;
     int* status;
     uint64_t limit_ns;
+    uint64_t hold_ns;           // testing hook: block 0 reaches its first barrier this late
     unsigned long long* trace;  // [kMaxRounds][kTraceWords] per-round timestamps and sizes
 };
 
@@ -480,6 +481,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             if (lane == 0 && lp) atomicAdd(tr + 6, lp);
         }
         if (__any_sync(0xFFFFFFFFu, offered) && lane == 0) a.ctr[5 + par] = 1u;
+        if (a.hold_ns && r == 0 && blockIdx.x == 0) {
+            // testing hook: block 0 arrives late (a bounded sleep), so the other
+            // blocks' barrier waits run out when hold_ns exceeds the limit
+            if (threadIdx.x == 0) {
+                const uint64_t t0 = global_ns();
+                while (global_ns() - t0 < a.hold_ns) __nanosleep(1000);
+            }
+            __syncthreads();
+        }
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[1] = global_ns();
         if (__ldcg(a.ctr + 5 + par) == 0u) break;
@@ -772,6 +782,7 @@ __global__ void k_tree_weight(const cs_edge* __restrict__ out, uint64_t cap, con
 struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
     bool labels = false;
+    uint64_t limit_ns = 0, hold_ns = 0;  // grid-barrier limit and test hold captured in the graph
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
     DevBuf mpts, parent, best, tree, live, wl, rlist, fl, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins,
         trace;
@@ -836,7 +847,8 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.ctr = p.ctr.as<uint32_t>();
     a.bar = p.bar.as<unsigned>();
     a.status = p.status.as<int>();
-    a.limit_ns = kBarrierLimitNs;
+    a.limit_ns = p.limit_ns;
+    a.hold_ns = p.hold_ns;
     return a;
 }
 
@@ -963,6 +975,8 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->block = block;
         p->flatten_div = flatten_div;
         p->labels = labels;
+        p->limit_ns = g.sweep_barrier_ns ? g.sweep_barrier_ns : kBarrierLimitNs;
+        p->hold_ns = g.sweep_hold_ns;
         p->key_ptrs[0] = g.eu.p;
         p->key_ptrs[1] = g.ev.p;
         p->key_ptrs[2] = g.ew.p;
@@ -1050,7 +1064,9 @@ void run_pass(Graph& g, SweepPlan& p) {
 
 bool plan_matches(const SweepPlan* p, const Graph& g, uint32_t K, uint32_t block, uint32_t fdiv, bool labels) {
     return p && p->n == g.n && p->E == g.e_total && p->e_knn == g.e_knn && p->K == K && p->block == block &&
-           p->flatten_div == fdiv && p->labels == labels && p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
+           p->flatten_div == fdiv && p->labels == labels &&
+           p->limit_ns == (g.sweep_barrier_ns ? g.sweep_barrier_ns : kBarrierLimitNs) && p->hold_ns == g.sweep_hold_ns &&
+           p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
            p->key_ptrs[2] == g.ew.p && p->key_ptrs[3] == g.dists.p && p->key_ptrs[4] == g.counts.p &&
            p->key_ptrs[5] == g.node_off.p;
 }
@@ -1127,7 +1143,8 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
     if (out_ms) *out_ms = ms;
 }
 
-void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res) {
+void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_labels, MstHost* res,
+                 bool device_out) {
     if (!g.plan) fail(CS_ERR_STATE, "sweep_fetch: no sweep has run");
     if (index >= g.sweep_K) fail(CS_ERR_INVALID, "sweep_fetch: index out of range");
     SweepPlan* p = g.plan;
@@ -1149,8 +1166,20 @@ void sweep_fetch(Graph& g, uint32_t index, cs_edge* out_edges, uint32_t* out_lab
     res->nedges = ne;
     res->ncomp = static_cast<uint32_t>(p->n - ne);
     res->weight = exact_sum_from_bins(bins);
-    if (out_edges && ne) copy_d2h(c, out_edges, p->out.as<cs_edge>() + j * cap, ne * sizeof(cs_edge));
-    if (out_labels && p->n) copy_d2h(c, out_labels, p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n, static_cast<uint64_t>(p->n) * 4);
+    const cs_edge* src_e = p->out.as<cs_edge>() + j * cap;
+    const uint32_t* src_l = p->labels ? p->lab.as<uint32_t>() + static_cast<uint64_t>(j) * p->n : nullptr;
+    if (device_out) {
+        // the caller's device buffers on this device, copied on the context stream
+        if (out_edges && ne)
+            CSB_CUDA(cudaMemcpyAsync(out_edges, src_e, ne * sizeof(cs_edge), cudaMemcpyDeviceToDevice, c.stream));
+        if (out_labels && p->n)
+            CSB_CUDA(cudaMemcpyAsync(out_labels, src_l, static_cast<uint64_t>(p->n) * 4, cudaMemcpyDeviceToDevice,
+                                     c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
+    if (out_edges && ne) copy_d2h(c, out_edges, src_e, ne * sizeof(cs_edge));
+    if (out_labels && p->n) copy_d2h(c, out_labels, src_l, static_cast<uint64_t>(p->n) * 4);
 }
 
 SweepOut sweep_outputs(Graph& g, uint32_t index) {
@@ -1214,7 +1243,19 @@ cs_status cs_sweep_fetch(cs_graph* gp, uint32_t index, cs_edge* out_edges, uint3
     Graph* g = reinterpret_cast<Graph*>(gp);
     return guarded(g ? g->ctx : nullptr, [&] {
         MstHost r;
-        sweep_fetch(*g, index, out_edges, out_labels, &r);
+        sweep_fetch(*g, index, out_edges, out_labels, &r, false);
+        if (out_nedges) *out_nedges = r.nedges;
+        if (out_ncomp) *out_ncomp = r.ncomp;
+        if (out_weight) *out_weight = r.weight;
+    });
+}
+
+cs_status cs_sweep_fetch_device(cs_graph* gp, uint32_t index, cs_edge* d_out_edges, uint32_t* d_out_labels,
+                                uint64_t* out_nedges, uint32_t* out_ncomp, double* out_weight) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        MstHost r;
+        sweep_fetch(*g, index, d_out_edges, d_out_labels, &r, true);
         if (out_nedges) *out_nedges = r.nedges;
         if (out_ncomp) *out_ncomp = r.ncomp;
         if (out_weight) *out_weight = r.weight;
@@ -1261,6 +1302,15 @@ cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t flatten_div, uint32_t block_
                     "cs_set_sweep_shape: block must be 128, 256 or 512");
         g->sweep_block = block_threads;
         g->sweep_flatten = flatten_div == 0 ? kFlattenAuto : (flatten_div == 0xFFFFFFFFu ? 0 : flatten_div);
+    });
+}
+
+cs_status cs_test_sweep_barrier(cs_graph* gp, uint64_t limit_ns, uint64_t hold_ns) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(hold_ns <= 5000000000ull, "cs_test_sweep_barrier: hold above 5 s");
+        g->sweep_barrier_ns = limit_ns;
+        g->sweep_hold_ns = hold_ns;
     });
 }
 
