@@ -1,11 +1,11 @@
-"""Multi-GPU mode of the extraction: independent replicas, one process per GPU.
+"""Process-group plumbing of the multi-GPU modes, one process per GPU.
 
-The K MSTs of a sweep, and whole sweeps, are independent: every rank holds its own
-resident CORE-SG in its own context and sweeps all K mpts on it (weak scaling).  No
-data crosses between ranks; torch.distributed is used only for the barriers around
-the timed region and for the maximum of the ranks' device times.  The backend is
-NCCL on GPUs (the reduction tensor lives on the rank's device) and gloo on the host
-(tests).
+Ranks from the torchrun environment, barriers, and the maximum (or sum) over ranks of
+a rank's device time.  The backend is NCCL on GPUs (the reduction tensor lives on the
+rank's device) and gloo on the host (tests).  The data path of a multi-GPU sweep --
+the CORE-SG broadcast, the mpts partition and the gather of the trees -- is in
+partition.py; replica_throughput is the throughput of independent replicas (every
+rank sweeping all K mpts of its own graph).
 """
 from __future__ import annotations
 
@@ -35,6 +35,16 @@ class Ranks:
 
         t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
         self.group.all_reduce(t, op=self.group.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(self, x: float) -> float:
+        """sum of x over all ranks (every rank gets it); x itself when alone."""
+        if self.group is None:
+            return float(x)
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.group.all_reduce(t, op=self.group.ReduceOp.SUM)
         return float(t.item())
 
     def close(self) -> None:
