@@ -22,6 +22,14 @@ Reported (one JSON line from rank 0):
   roofline   the persistent Boruvka kernel against the measured HBM copy bandwidth
   cpu_baseline  the reference CPU extract (built from its sources) on the same
              CORE-SG, a bounded sample of mpts values, all host threads
+  parity     the sweep's trees against the reference's own CoreSG::mst on the same
+             CORE-SG for the baseline's mpts values (edges, weight bits, labels,
+             components, exact weight)
+  build_roofline  the descent's FP32 rate (3 d FLOP per distance evaluation) against
+             the CUDA-core FP32 peak at the sampled SM clock
+With --gpus N > 1 (torchrun, one rank per GPU) a step is one sweep of mpts 1..K
+partitioned across the ranks plus the gather of all K results into rank 0's device
+memory (run_partitioned; strong scaling).
 Inputs: seeded synthetic Gaussian mixtures with the workload's shapes; the edge list
 (12 B x |E|, ~300 MB at n=1M) is larger than L2, so no L2 flush is needed.
 """
@@ -62,12 +70,18 @@ def profiled_traffic(workload: str, n: int):
 def build_recall(g, pts, device: int, queries: int, seed: int) -> dict:
     """recall@k of the resident k-NN graph against FP32 brute force for a seeded sample
     of query points (torch on the device, chunks of 500 queries; a measurement only)."""
+    ids, _, _, counts = g.knn()
+    return recall_of(ids, counts, pts, device, queries, seed)
+
+
+def recall_of(ids, counts, pts, device: int, queries: int, seed: int) -> dict:
+    """recall@k of k-NN arrays (ids [n][k], counts [n]) against FP32 brute force for a
+    seeded sample of query points (torch.cdist on the device, 500 queries a chunk)."""
     import torch
 
-    n, k = len(pts), g.k_max
+    n, k = ids.shape
     rng = np.random.default_rng(seed)
     q = np.sort(rng.choice(n, size=min(queries, n), replace=False))
-    ids, _, _, counts = g.knn()
     X = torch.from_numpy(np.ascontiguousarray(pts, np.float32)).to(f"cuda:{device}")
     hits = total = 0
     for c0 in range(0, len(q), 500):
@@ -83,7 +97,53 @@ def build_recall(g, pts, device: int, queries: int, seed: int) -> dict:
     del X
     torch.cuda.empty_cache()
     return {"recall_at_k": hits / total, "k": k, "queries": int(len(q)),
-            "what": "k-NN lists of the device build vs FP32 brute force (torch.cdist), sampled queries"}
+            "what": "k-NN lists vs FP32 brute force (torch.cdist), sampled queries"}
+
+
+def reference_gpu_build(cs, ctx, device, pts, w):
+    """The reference's own CUDA NN-Descent (coresg::cuda::nndescent_gpu, its sources
+    built for sm_100a with its flags by oracle/Makefile) on this workload, once, as
+    CudaBackend::run_knn_job runs it: host buffers in and out, its device allocations
+    included (sample 16, 10 iterations, delta 0.001); beside it, the engine's
+    cs_nndescent at the same boundary.  Wall seconds and recall@k of each."""
+    import ctypes as C
+
+    from coresg_b200.datagen import pad_rows
+
+    so = os.path.join(ROOT, "oracle", "_ref", "libcoresg_refgpu.so")
+    if not os.path.exists(so):
+        return {"unavailable": "oracle/_ref/libcoresg_refgpu.so (the reference's CUDA sources built) is missing"}
+    lib = C.CDLL(so)
+    lib.refgpu_last_error.restype = C.c_char_p
+    P, U32, U64 = C.c_void_p, C.c_uint32, C.c_uint64
+    lib.refgpu_nndescent.argtypes = [C.c_int, U32, U32, U32, U32, U32, U32, U64, C.c_int, C.c_float,
+                                     P, P, P, P, P, P]
+    padded = pad_rows(pts)
+    n, stride = padded.shape
+    k = w["k_max"]
+    ids = np.full((n, k), 0xFFFFFFFF, np.uint32)
+    dists = np.full((n, k), np.inf, np.float32)
+    flags = np.zeros((n, k), np.uint8)
+    counts = np.zeros(n, np.uint32)
+    upd = C.c_uint64()
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    t0 = time.perf_counter()
+    rc = lib.refgpu_nndescent(device, n, w["dim"], stride, k, 16, 10, 42, 0, 0.001, ptr(padded), ptr(ids),
+                              ptr(dists), ptr(flags), ptr(counts), C.byref(upd))
+    ref_s = time.perf_counter() - t0
+    if rc:
+        return {"failed": lib.refgpu_last_error().decode()}
+    ref_recall = recall_of(ids, counts, pts, device, 10000, 7)["recall_at_k"]
+    t0 = time.perf_counter()
+    mids, _, _, mcounts, _ = ctx.nndescent(padded, k=k, sample=16, iters=10, seed=42)
+    ours_s = time.perf_counter() - t0
+    ours_recall = recall_of(mids, mcounts, pts, device, 10000, 7)["recall_at_k"]
+    return {"reference_nndescent_gpu_s": ref_s, "reference_recall_at_k": ref_recall,
+            "engine_cs_nndescent_s": ours_s, "engine_recall_at_k": ours_recall,
+            "speedup": ref_s / ours_s if ours_s > 0 else None,
+            "what": "the reference's cuda::nndescent_gpu (built for sm_100a) vs the engine's cs_nndescent, host "
+                    "buffers in and out, sample 16, 10 iterations, same B200; recall vs FP32 brute force, 10,000 "
+                    "sampled queries"}
 
 
 def log(*a):
@@ -167,6 +227,12 @@ def sweep_kernel_bytes(n, E, K):
     return 12 * E + 4 * 32 * n + 4 * E * passes
 
 
+def config_of(name, w):
+    """The workload description both arms print."""
+    return {"workload": name, "n": w["n"], "dim": w["dim"], "k_max": w["k_max"], "mpts": f"1..{w['k_max']}",
+            "l2": "inputs larger than L2 (edge list 12 B x |E|), no flush"}
+
+
 # ---------------------------------------------------------------------------------------
 
 def run_reference(args):
@@ -204,8 +270,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / len(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "n": w["n"], "dim": w["dim"], "k_max": w["k_max"],
-                   "step": "one CoreSG::mst(mpts) all-in, mpts cycling 1..k_max"},
+        "config": config_of(args.workload, w),
+        "step": "one CoreSG::mst(mpts) all-in, mpts cycling 1..k_max",
         "build_s": build_s,
         "cpu_baseline": {"value": value, "unit": "MSTs/s", "cores": cores, "kind": "reference",
                          "sample": f"{len(secs)} extractions (mpts {mp[args.warmup]}..), CoreSG::mst all-in"},
@@ -216,24 +282,66 @@ def run_reference(args):
 
 
 def cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges):
-    """The reference CPU extract on this CORE-SG (a bounded sample of mpts)."""
+    """The reference CPU extract on this CORE-SG (a bounded sample of mpts).  Returns
+    the baseline and the reference's trees ({mpts: CoreSG::mst result}) for the
+    parity check, or (None, {})."""
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         from checkers import Reference
         from coresg_b200.datagen import pad_rows
 
         if not Reference.available():
-            return None
+            return None, {}
         ref = Reference()
         sg = ref.from_state(pad_rows(pts), w["dim"], ids, dists, flags, counts, bridges, threads=0)
         sample = [1, 8, 16, w["k_max"]]
-        secs = [sg.mst(m, algo=0)["seconds_all"] for m in sample]
-        return {"value": len(sample) / sum(secs), "unit": "MSTs/s", "cores": os.cpu_count() or 1,
-                "kind": "reference",
-                "sample": f"CoreSG::mst all-in for mpts {sample} on this CORE-SG ({sum(secs):.1f} s)"}
+        trees = {m: sg.mst(m, algo=0) for m in sample}
+        secs = [trees[m]["seconds_all"] for m in sample]
+        return ({"value": len(sample) / sum(secs), "unit": "MSTs/s", "cores": os.cpu_count() or 1,
+                 "kind": "reference",
+                 "sample": f"CoreSG::mst all-in for mpts {sample} on this CORE-SG ({sum(secs):.1f} s)"}, trees)
     except Exception as e:  # the baseline is reported, never required
         log(f"[cpu_baseline] failed: {e}")
-        return None
+        return None, {}
+
+
+def parity_at_scale(g, mpts, ref_trees):
+    """The engine's batched sweep against the reference's own CoreSG::mst on the same
+    CORE-SG, for the mpts values the CPU baseline solved: the tree edges (as sorted
+    (u, v) keys), the sorted weight bits, the labels and component count, the exact
+    weight of the reference tree (canonical sum, bit for bit) and the reference's own
+    double sum (within its reassociation error)."""
+    if not ref_trees:
+        return {"checked": False, "why": "reference CPU path unavailable"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from checkers import Oracle
+
+    orc = Oracle()
+    g.sweep_device(mpts)
+    n = g.n
+
+    def keys(e):
+        return np.sort((e["u"].astype(np.uint64) << np.uint64(32)) | e["v"].astype(np.uint64))
+
+    per = []
+    for m, r in sorted(ref_trees.items()):
+        mine = g.sweep_fetch(mpts.index(m))
+        same_len = len(mine.edges) == len(r["edges"])
+        chk = {
+            "mpts": m, "tree_edges": int(len(mine.edges)),
+            "edges": bool(same_len and np.array_equal(keys(mine.edges), keys(r["edges"]))),
+            "weight_bits": bool(same_len and np.array_equal(np.sort(mine.edges["w"]).view(np.uint32),
+                                                            np.sort(r["edges"]["w"]).view(np.uint32))),
+            "labels": bool(np.array_equal(mine.component, r["labels"])),
+            "components": bool(mine.num_components == r["ncomp"]),
+            "exact_weight": bool(mine.weight == orc.exact_sum(r["edges"]["w"])),
+            "reference_weight_rel": abs(mine.weight - r["weight"]) / max(1.0, abs(r["weight"])),
+        }
+        chk["equal"] = all(chk[x] for x in ("edges", "weight_bits", "labels", "components", "exact_weight"))
+        per.append(chk)
+    return {"checked": True, "mpts": sorted(ref_trees), "equal": all(c["equal"] for c in per), "per_mpts": per,
+            "what": "batched sweep vs the reference CoreSG::mst on the same CORE-SG: tree edges, weight bits, "
+                    "labels, components, exact weight"}
 
 
 def run_inserts(cs, ctx, args):
@@ -244,7 +352,7 @@ def run_inserts(cs, ctx, args):
     batches and the stages of each."""
     from coresg_b200.datagen import insert_batch, workload
 
-    pts, w = workload(args.insert_workload)
+    pts, w = workload(args.insert_workload, args.insert_n)
     g = cs.CoreSG(ctx, w["dim"], w["k_max"])
     rng = np.random.default_rng(w["seed"] + 1)
     sizes = [int(x) for x in rng.integers(10_000, 200_001, size=args.insert_batches)]
@@ -264,8 +372,11 @@ def run_inserts(cs, ctx, args):
         st = g.insert_stats()
         secs += dt
         rows += len(b)
+        bs = g.bridge_stats()
         per.append({"rows": len(b), "ms": round(1000 * dt, 2),
-                    **{k: round(v, 2) for k, v in st.items() if k.endswith("_ms") and k != "total_ms"}})
+                    **{k: round(v, 2) for k, v in st.items() if k.endswith("_ms") and k != "total_ms"},
+                    "bridge_stages_ms": {k[:-3]: round(v, 3) for k, v in bs.items()
+                                         if k.endswith("_ms") and k != "total_ms"}})
     n_end = g.n
     g.close()
     return {"workload": args.insert_workload, "n_start": w["n"], "n_end": int(n_end), "k_max": w["k_max"],
@@ -374,6 +485,155 @@ def run_e2e(cs, ctx, g, mpts, arrays, steps, inflight, max_over_ranks, world, sh
             "d2h_bytes_per_step": int(d2h[0]), "steps": steps * len(graphs), "inflight": len(graphs),
             "serial": {"value": world * K * steps / serial_s, "steps": steps},
             "what": f"cs_graph_set_knn + cs_graph_set_bridges + cs_extract_sweep (trees and labels) per step, page-locked host buffers; {len(graphs)} graph(s) on their own contexts in flight"}
+
+
+def run_partitioned(cs, args, ranks):
+    """--gpus N > 1: one CORE-SG on N GPUs (coresg_b200/partition.py).  Rank 0 builds
+    the workload's CORE-SG on its GPU and its state (k-NN arrays and bridges) is
+    broadcast over NCCL, so every rank holds the same graph.  A step is one sweep of
+    mpts 1..K split across the ranks (rank r sweeps positions r, r + N, ...) followed by
+    the gather of every tree, label array and scalar triple into rank 0's device memory
+    (NCCL gather).  Each rank times its steps with CUDA events on its engine stream,
+    which the fetch and the gather run on too; the job's time is the maximum over
+    ranks, and value = K MSTs per step over it (strong scaling: the work per step is
+    fixed as N grows).  Rank 0 then checks the gathered results against a one-GPU
+    sweep of all K on its own graph."""
+    import torch
+
+    from coresg_b200 import partition
+    from coresg_b200.datagen import workload
+
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    dist = ranks.group
+    dev = f"cuda:{local}"
+    ctx = cs.Context(local)
+    pts, w = workload(args.workload, args.n)
+    n, K = w["n"], w["k_max"]
+    mpts = list(range(1, K + 1))
+    g = cs.CoreSG(ctx, w["dim"], K)
+    state, build_s = None, None
+    if rank == 0:
+        t0 = time.perf_counter()
+        g.build(pts, sample=16, iters=10, delta=0.001, seed=42)
+        build_s = time.perf_counter() - t0
+        ids, dists, flags, counts = g.knn()
+        state = [ids, dists, flags, counts, g.missing_edges().view(np.uint32)]
+    ranks.barrier()
+    t0 = time.perf_counter()
+    got = partition.broadcast_arrays(dist, state, dev)
+    torch.cuda.synchronize(dev)
+    replicate_s = ranks.max_over_ranks(time.perf_counter() - t0)
+    state_bytes = sum(a.nbytes for a in got)
+    if rank != 0:
+        g.set_knn(*got[:4])
+        g.set_bridges(got[4].view(cs.EDGE_DTYPE))
+    info = g.info()
+    E = info["knn_edges"] + info["bridges"]
+    pos = partition.share_positions(K, world, rank)
+    mine = [mpts[j] for j in pos]
+    bufs = partition.ResultBuffers(partition.max_share(K, world), n, dev)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    gathered = [None]
+
+    def step():
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            ev0.record(ext)
+            if mine:
+                g.sweep_device(mine)
+                partition.fetch_share(g, range(len(mine)), bufs)
+            gathered[0] = partition.gather_results(dist, K, bufs)
+            ev1.record(ext)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    for _ in range(args.warmup):
+        step()
+    clk = Clocks(local, args.clocks_dir)
+    ranks.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = ctx.launches
+    clk.start()
+    ms = [step() for _ in range(args.steps)]
+    clocks = clk.stop()
+    launches = ranks.sum_over_ranks(ctx.launches - launches0)
+    ranks.barrier()
+    total_ms = ranks.max_over_ranks(sum(ms))
+    value = K * args.steps / (total_ms / 1000.0)
+    sweep_ms = ranks.max_over_ranks(float(np.mean([g.sweep_timing()[0]])) if mine else 0.0)
+
+    check = None
+    if rank == 0:
+        edges, labels, scalars = gathered[0]
+        alone = g.all_msts(mpts)
+        ok = True
+        for j, r in enumerate(alone):
+            ne = int(scalars[j, 0])
+            ok &= ne == len(r.edges) and int(scalars[j, 1]) == r.num_components
+            ok &= float(scalars[j, 2]) == r.weight
+            ok &= partition.unpack(edges[j], ne).tobytes() == r.edges.tobytes()
+            ok &= np.array_equal(labels[j].cpu().numpy().view(np.uint32), r.component)
+        check = {"equal": bool(ok), "what": "gathered trees, labels and scalars vs a one-GPU sweep of all K "
+                                            "on rank 0's graph"}
+    gather_bytes = (world - 1) * bufs.L * (bufs.edges[0].numel() * 4 + bufs.labels[0].numel() * 4 + 24)
+
+    # e2e through the public API: every rank uploads the CORE-SG from page-locked host
+    # arrays (cs_graph_set_knn + cs_graph_set_bridges) and extracts its share into
+    # page-locked host outputs (cs_extract_sweep); wall time, max over ranks
+    e2e = None
+    if args.e2e_steps > 0 and mine:
+        host = [cs.Pinned(a.shape, a.dtype) for a in got]
+        for p_, a in zip(host, got):
+            p_.array[...] = a
+        oe = cs.Pinned((len(mine), max(n - 1, 1)), cs.EDGE_DTYPE)
+        ol = cs.Pinned((len(mine), n), np.uint32)
+
+        def e2e_step():
+            g.set_knn(*(p_.array for p_ in host[:4]))
+            g.set_bridges(host[4].array.view(cs.EDGE_DTYPE))
+            return g.all_msts(mine, labels=True, out_edges=oe.array, out_labels=ol.array)
+
+        e2e_step()
+        ranks.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            res = e2e_step()
+        e2e_s = ranks.max_over_ranks(time.perf_counter() - t0)
+        d2h = ranks.sum_over_ranks(sum(r.edges.nbytes + r.component.nbytes + 20 for r in res))
+        e2e = {"value": K * args.e2e_steps / e2e_s, "unit": "MSTs/s",
+               "h2d_bytes_per_step": int(world * state_bytes), "d2h_bytes_per_step": int(d2h),
+               "steps": args.e2e_steps,
+               "what": "every rank: cs_graph_set_knn + cs_graph_set_bridges from page-locked host arrays and "
+                       "cs_extract_sweep of its mpts share into page-locked host outputs"}
+        for p_ in host + [oe, ol]:
+            p_.free()
+    elif args.e2e_steps > 0:
+        # a rank without a share still takes the same collective steps
+        ranks.barrier()
+        ranks.max_over_ranks(0.0)
+        ranks.sum_over_ranks(0.0)
+    if rank == 0:
+        peak, peak_kind = peaks()
+        line = {
+            "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(args.workload, w),
+            "graph": {"edges": E, "knn_edges": info["knn_edges"], "bridges": info["bridges"]},
+            "multi_gpu": {"mode": "mpts partition + gather to rank 0", "ranks": world,
+                          "mpts_per_rank": [len(partition.share_positions(K, world, r)) for r in range(world)],
+                          "replicate_s": replicate_s, "replicated_bytes": int(state_bytes),
+                          "gather_bytes_per_step": int(gather_bytes), "sweep_ms_max_over_ranks": sweep_ms,
+                          "check": check},
+            "build_s": build_s, "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "roofline": None, "cpu_baseline": None,
+            "roofline_note": f"see the one-GPU line; peak source {peak_kind} {peak} GB/s",
+        }
+        print(json.dumps(line))
+    del bufs, gathered
+    g.close()
+    ranks.close()
+    return 0
 
 
 def run_serving(cs, ctx, args):
@@ -496,7 +756,10 @@ def main():
     ap.add_argument("--serve-inserts-first", type=int, default=1)
     ap.add_argument("--insert-workload", default="blobs2m_d32")
     ap.add_argument("--insert-batches", type=int, default=16, help="insert leg batches (0: skip)")
+    ap.add_argument("--insert-n", type=int, default=None, help="override the insert workload's base point count")
     ap.add_argument("--highdim", type=int, default=1, help="d=128 f32/u8 build leg (0: skip)")
+    ap.add_argument("--ref-gpu", type=int, default=1,
+                    help="time the reference's own CUDA NN-Descent (built for sm_100a) once (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -506,7 +769,9 @@ def main():
     from coresg_b200 import replicas
     from coresg_b200.datagen import workload
 
-    ranks = replicas.from_env("nccl")
+    ranks = replicas.from_env("nccl", timeout_s=300)
+    if ranks.world > 1:
+        return run_partitioned(cs, args, ranks)
     world, rank, local = ranks.world, ranks.rank, ranks.local
     barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
@@ -524,11 +789,11 @@ def main():
     warm.close()
     first_use_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42 + rank)
+    st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42)
     build_s = time.perf_counter() - t0
     # the same build again on the same resident graph: no fresh device allocations
     t0 = time.perf_counter()
-    st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42 + rank)
+    st = g.build(pts, sample=16, iters=10, delta=0.001, seed=42)
     rebuild_s = time.perf_counter() - t0
     bstats = g.build_stats()
     d_pts = w["dim"]
@@ -566,6 +831,10 @@ def main():
     ms_per_step = total_ms / args.steps
     kernel_ms = float(np.mean(kern_ms))
     log(f"[rank {rank}] sweep {ms_per_step:.3f} ms/step (kernel {kernel_ms:.3f} ms) wall {wall:.3f}s")
+    # per-round profile of the last timed sweep's persistent kernel (cs_sweep_trace)
+    trace = [{"phase_a_ms": int(t[0]) / 1e6, "phase_b_ms": int(t[1]) / 1e6, "flatten_ms": int(t[2]) / 1e6,
+              "edges": int(t[3]), "roots": int(t[4]), "full_flatten": int(t[5]), "live_pairs": int(t[6])}
+             for t in g.sweep_trace()]
 
     # ---- plain per-mpts path on the same graph (one pass over 1..K)
     plain = None
@@ -606,9 +875,27 @@ def main():
                 "sweep_graph": {"algorithmic_bytes": sweep_bytes(n, E, K), "ms": ms_per_step,
                                 "achieved_gbs": sweep_bytes(n, E, K) / (ms_per_step / 1000.0) / 1e9}}
 
-    cpu = None
+    # ---- the build's FP32 roofline: 3 d FLOP per distance evaluation of the local
+    # joins (NNDescentStats::distance_evals) over the descent's device time (sample,
+    # join and merge kernels of every round), against the FP32 CUDA-core peak at the
+    # SM clock sampled during the sweep (128 FP32 lanes x 2 FLOP per SM per cycle)
+    sm_count = cs.device_props(local)["sm_count"]
+    clk_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    fp32_peak = sm_count * 128 * 2 * clk_mhz * 1e6 / 1e12
+    build_roofline = {"bound": "fp32", "achieved": bstats["gflops"] / 1e3, "peak": fp32_peak, "unit": "TFLOP/s",
+                      "frac": bstats["gflops"] / 1e3 / fp32_peak,
+                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x 2 FLOP x {clk_mhz:.0f} MHz (sampled)",
+                      "what": "3 d x distance evaluations over the descent's device time (sample + join + merge)"}
+
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges)
+        cpu, ref_trees = cpu_baseline(g, pts, w, ids, dists, flags, counts, bridges)
+        parity = parity_at_scale(g, mpts, ref_trees)
+        log(f"[rank {rank}] parity at n={n}: {parity.get('equal')}")
+    ref_gpu = None
+    if rank == 0 and world == 1 and args.ref_gpu:
+        ref_gpu = reference_gpu_build(cs, ctx, local, pts, w)
+        log(f"[rank {rank}] reference GPU build {ref_gpu}")
 
     serving = inserts = highdim = None
     g.close()
@@ -630,11 +917,15 @@ def main():
             "metric": METRIC, "value": value, "unit": "MSTs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "n": n, "dim": w["dim"], "k_max": K, "mpts": f"1..{K}",
-                       "edges": E, "knn_edges": info["knn_edges"], "bridges": info["bridges"],
-                       "sweep_flatten_div": flatten, "sweep_block": block,
-                       "l2": "inputs larger than L2 (edge list 12 B x |E|), no flush"},
+            "config": config_of(args.workload, w),
+            "graph": {"edges": E, "knn_edges": info["knn_edges"], "bridges": info["bridges"]},
+            "sweep_shape": {"flatten_div": flatten, "block": block},
+            "sweep_trace": trace,
+            "parity": parity,
             "build_s": build_s, "rebuild_s": rebuild_s, "build": st, "build_device": bstats,
+            "build_roofline": build_roofline,
+            "build_reference_gpu": ref_gpu,
+            "build_reference_gpu_s": (ref_gpu or {}).get("reference_nndescent_gpu_s"),
             "build_recall": recall, "first_use_s": first_use_s,
             "plain": plain, "speedup_vs_plain": (value / world) / plain["value"] if plain else None,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
