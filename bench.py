@@ -376,7 +376,8 @@ def run_inserts(cs, ctx, args):
         per.append({"rows": len(b), "ms": round(1000 * dt, 2),
                     **{k: round(v, 2) for k, v in st.items() if k.endswith("_ms") and k != "total_ms"},
                     "bridge_stages_ms": {k[:-3]: round(v, 3) for k, v in bs.items()
-                                         if k.endswith("_ms") and k != "total_ms"}})
+                                         if k.endswith("_ms") and k != "total_ms"},
+                    "hub_refreshed": bs["hub_refreshed"], "rescored": bs["rescored"]})
     n_end = g.n
     g.close()
     return {"workload": args.insert_workload, "n_start": w["n"], "n_end": int(n_end), "k_max": w["k_max"],

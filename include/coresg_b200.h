@@ -254,14 +254,22 @@ cs_status cs_select_bridges(cs_graph* g, uint64_t* out_selected, uint64_t* out_b
  * (include/coresg/hubness.hpp:121-142) split the reference's build. */
 typedef struct {
     double connectivity_ms;  /* union-find over the k-NN lists, dense component labels */
-    double hubness_ms;       /* reverse degrees and scores */
+    double hubness_ms;       /* reverse degrees and scores: after the first selection on a graph, an
+                                incremental refresh (the deltas of the lists that changed since, and
+                                the nodes whose score inputs moved rescored) */
     double edges_ms;         /* the undirected k-NN edge list (its count is the budget's |E|) */
     double selection_ms;     /* budget-lowest selection, per-component quota, ordering */
     double bridge_mst_ms;    /* dense MRD + Prim over the selected anti-hubs */
     double repair_ms;        /* connectivity repair (0 when the bridges join every component) */
     double total_ms;
     uint64_t selected, bridges, repair;
-    uint32_t knn_components, reserved0;
+    uint32_t knn_components;
+    uint32_t hub_refreshed;  /* 1: the hubness stage was the incremental refresh (HubnessIndex::refresh,
+                                src/hubness.cpp:523-544); 0: a full pass (rescore_all) */
+    uint64_t rescored;       /* nodes whose score the hubness stage computed */
+    uint64_t changed;        /* nodes whose list changed since the last scoring (n after a full
+                                pass with no earlier state); the refresh runs when at most n / 16
+                                changed, else a full pass is the cheaper one */
 } cs_bridge_stats;
 cs_status cs_bridge_stats_get(cs_graph* g, cs_bridge_stats* out);
 /* The selected anti-hubs of the last cs_select_bridges (HubnessIndex::selected). */

@@ -246,7 +246,8 @@ class BridgeStats(C.Structure):
     _fields_ = [("connectivity_ms", C.c_double), ("hubness_ms", C.c_double), ("edges_ms", C.c_double),
                 ("selection_ms", C.c_double), ("bridge_mst_ms", C.c_double), ("repair_ms", C.c_double),
                 ("total_ms", C.c_double), ("selected", C.c_uint64), ("bridges", C.c_uint64), ("repair", C.c_uint64),
-                ("knn_components", C.c_uint32), ("reserved0", C.c_uint32)]
+                ("knn_components", C.c_uint32), ("hub_refreshed", C.c_uint32), ("rescored", C.c_uint64),
+                ("changed", C.c_uint64)]
 
 
 class MstResult:
@@ -379,7 +380,7 @@ class CoreSG:
         """Stages of the last bridge selection (cs_bridge_stats_get)."""
         x = BridgeStats()
         self.ctx.check(lib().cs_bridge_stats_get(self.h, C.byref(x)))
-        return {name: getattr(x, name) for name, _ in BridgeStats._fields_ if name != "reserved0"}
+        return {name: getattr(x, name) for name, _ in BridgeStats._fields_}
 
     def selected(self):
         cnt = C.c_uint64(0)

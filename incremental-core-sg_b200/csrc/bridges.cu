@@ -45,15 +45,36 @@ __global__ void k_iota_u32(uint32_t* __restrict__ a, uint32_t n) {
     if (i < n) a[i] = i;
 }
 
-/// Unite every node with each of its listed neighbours.
+/// Unite every node with its listed neighbours at list positions [j0, j1).
 __global__ void k_conn_unite(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n,
-                             uint32_t k, uint32_t* __restrict__ parent, int* status) {
+                             uint32_t k, uint32_t j0, uint32_t j1, uint32_t* __restrict__ parent, int* status) {
+    const uint32_t span = j1 - j0;
     const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= static_cast<uint64_t>(n) * k) return;
-    const uint32_t p = static_cast<uint32_t>(t / k), j = static_cast<uint32_t>(t % k);
+    if (t >= static_cast<uint64_t>(n) * span) return;
+    const uint32_t p = static_cast<uint32_t>(t / span), j = j0 + static_cast<uint32_t>(t % span);
     if (j >= counts[p]) return;
-    const uint32_t q = ids[t];
+    const uint32_t q = ids[static_cast<uint64_t>(p) * k + j];
     if (q < n && q != p) uf_unite(parent, p, q, n, status);
+}
+
+/// Point every node at its root (no unions run meanwhile, so a chase that meets an
+/// entry another thread rewrote still ends at the same root).  A chase longer than
+/// n (a cycle, which the linking rule rules out) sets the status and stops.
+__global__ void k_compress(uint32_t* __restrict__ parent, uint32_t n, int* status) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    uint32_t r = __ldcg(parent + v);
+    if (r == v) return;
+    for (uint32_t it = 0;; ++it) {
+        const uint32_t p = __ldcg(parent + r);
+        if (p == r) break;
+        if (it > n) {
+            atomicOr(status, kStatusUnionLimit);
+            return;
+        }
+        r = p;
+    }
+    parent[v] = r;
 }
 
 __global__ void k_rdeg(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
@@ -66,12 +87,13 @@ __global__ void k_rdeg(const uint32_t* __restrict__ ids, const uint32_t* __restr
     if (q < n) atomicAdd(rdeg + q, 1);
 }
 
-/// compute_score, arithmetic mean (src/hubness.cpp:302-352); IEEE double division.
-__global__ void k_score(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
-                        uint32_t k_for_score, const int* __restrict__ rdeg, double* __restrict__ score,
-                        unsigned long long* __restrict__ key_score, unsigned long long* __restrict__ key_tie) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
+/// compute_score, arithmetic mean (src/hubness.cpp:302-352), of node v; IEEE double
+/// division.  Writes the score and v's selection keys.
+__device__ __forceinline__ void score_node(uint32_t v, const uint32_t* __restrict__ ids,
+                                           const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
+                                           uint32_t k_for_score, const int* __restrict__ rdeg,
+                                           double* __restrict__ score, unsigned long long* __restrict__ key_score,
+                                           unsigned long long* __restrict__ key_tie) {
     const uint32_t deg = counts[v];
     const int rd = rdeg[v];
     long long sum = 0;
@@ -92,6 +114,114 @@ __global__ void k_score(const uint32_t* __restrict__ ids, const uint32_t* __rest
     // scores are >= 0, so their bit patterns order like the values
     key_score[v] = static_cast<unsigned long long>(__double_as_longlong(s));
     key_tie[v] = (static_cast<unsigned long long>(static_cast<uint32_t>(rd)) << 32) | v;
+}
+
+__global__ void k_score(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n, uint32_t k,
+                        uint32_t k_for_score, const int* __restrict__ rdeg, double* __restrict__ score,
+                        unsigned long long* __restrict__ key_score, unsigned long long* __restrict__ key_tie) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    score_node(v, ids, counts, n, k, k_for_score, rdeg, score, key_score, key_tie);
+}
+
+// ---- incremental hubness refresh (HubnessIndex::refresh, src/hubness.cpp:523-544) ----
+// After a full pass the graph keeps a snapshot of the lists it scored.  k_merge flags
+// every node whose membership changed since (hub_changed); nodes added since the
+// snapshot count as changed.  The refresh applies the reverse-degree deltas of the
+// changed lists (on_edge_added / on_edge_removed, :242-279) and rescores exactly the
+// nodes whose score inputs moved: a changed list, a changed own reverse degree, or a
+// listed neighbour whose reverse degree changed (collect_rescore_set, :482-520, with the
+// reverse neighbours found by scanning the lists against the dirty flags).
+
+/// One node of k_hub_delta (warp-collective).
+__device__ __forceinline__ void hub_delta_node(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts,
+                                               uint32_t n, uint32_t k, uint32_t n_prev, uint32_t p, unsigned lane,
+                                               uint32_t* __restrict__ prev_ids, uint32_t* __restrict__ prev_cnt,
+                                               int* __restrict__ rdeg, uint8_t* __restrict__ rd_dirty) {
+    const bool fresh = p >= n_prev;
+    const uint32_t cn = counts[p], co = fresh ? 0u : prev_cnt[p];
+    const uint64_t base = static_cast<uint64_t>(p) * k;
+    uint32_t nw[2], od[2];
+    bool od_kept[2] = {false, false}, nw_known[2] = {false, false};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const uint32_t j = lane + 32u * e;
+        nw[e] = j < cn ? ids[base + j] : kInvalid;
+        od[e] = j < co ? prev_ids[base + j] : kInvalid;
+    }
+    const int halves = k > 32 ? 2 : 1;
+    for (int e2 = 0; e2 < halves; ++e2) {
+        for (int src = 0; src < 32; ++src) {
+            const uint32_t a = __shfl_sync(0xFFFFFFFFu, nw[e2], src);
+            const uint32_t b = __shfl_sync(0xFFFFFFFFu, od[e2], src);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                if (od[e] != kInvalid && od[e] == a) od_kept[e] = true;
+                if (nw[e] != kInvalid && nw[e] == b) nw_known[e] = true;
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        if (od[e] != kInvalid && !od_kept[e] && od[e] < n) {
+            atomicSub(rdeg + od[e], 1);
+            rd_dirty[od[e]] = 1;
+        }
+        if (nw[e] != kInvalid && !nw_known[e] && nw[e] < n) {
+            atomicAdd(rdeg + nw[e], 1);
+            rd_dirty[nw[e]] = 1;
+        }
+        const uint32_t j = lane + 32u * e;
+        if (j < k) prev_ids[base + j] = nw[e];
+    }
+    if (lane == 0) prev_cnt[p] = cn;
+}
+
+/// The nodes whose lists changed since the snapshot (flagged by k_merge, or added
+/// since: v >= n_prev), compacted into list[0..*cnt) with one atomic per warp.
+__global__ void k_hub_changed_list(uint32_t n, uint32_t n_prev, const uint8_t* __restrict__ changed,
+                                   uint32_t* __restrict__ list, uint32_t* __restrict__ cnt) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool want = v < n && (v >= n_prev || changed[v]);
+    const uint32_t at = warp_append(want, cnt);
+    if (want) list[at] = v;
+}
+
+/// Reverse-degree deltas of each listed node p's list against its snapshot, one warp
+/// per node (grid-stride over list[0..*cnt)): an id that left the list loses one
+/// reverse neighbour, an id that joined gains one; both get rd_dirty.  The snapshot
+/// takes the new list.  k <= 64 (two entries a lane).
+__global__ void k_hub_delta(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n,
+                            uint32_t k, uint32_t n_prev, const uint32_t* __restrict__ list,
+                            const uint32_t* __restrict__ cnt, uint32_t* __restrict__ prev_ids,
+                            uint32_t* __restrict__ prev_cnt, int* __restrict__ rdeg, uint8_t* __restrict__ rd_dirty) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t total = *cnt;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total; w += (gridDim.x * blockDim.x) >> 5) {
+        hub_delta_node(ids, counts, n, k, n_prev, list[w], lane, prev_ids, prev_cnt, rdeg, rd_dirty);
+    }
+}
+
+
+/// Rescore the nodes whose score inputs moved (see above); counts them into *rescored.
+__global__ void k_score_refresh(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ counts, uint32_t n,
+                                uint32_t k, uint32_t k_for_score, uint32_t n_prev, const uint8_t* __restrict__ changed,
+                                const uint8_t* __restrict__ rd_dirty, const int* __restrict__ rdeg,
+                                double* __restrict__ score, unsigned long long* __restrict__ key_score,
+                                unsigned long long* __restrict__ key_tie, unsigned long long* __restrict__ rescored) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    bool need = false;
+    if (v < n) {
+        need = v >= n_prev || changed[v] || rd_dirty[v];
+        const uint32_t deg = counts[v];
+        for (uint32_t j = 0; j < deg && !need; ++j) {
+            const uint32_t q = ids[static_cast<uint64_t>(v) * k + j];
+            need = q < n && rd_dirty[q];
+        }
+        if (need) score_node(v, ids, counts, n, k, k_for_score, rdeg, score, key_score, key_tie);
+    }
+    const unsigned b = __ballot_sync(0xFFFFFFFFu, need);
+    if ((threadIdx.x & 31u) == 0 && b) atomicAdd(rescored, static_cast<unsigned long long>(__popc(b)));
 }
 
 /// Histogram of one 8-bit digit of key[] over the elements whose higher digits
@@ -326,13 +456,15 @@ uint64_t antihub_budget(uint64_t num_edges, uint32_t dim, uint64_t n) {
 }
 
 /// The node-proportional selection scratch for `ns` nodes.
-void size_bridge_scratch(Scratch& s, uint64_t ns) {
+void size_bridge_scratch(Scratch& s, uint64_t ns, cudaStream_t st) {
     s.parent.ensure(ns * 4ull);
     s.lab.ensure(ns * 4ull);
-    s.rdeg.ensure(ns * 4ull);
-    s.score.ensure(ns * 8ull);
-    s.ks.ensure(ns * 8ull);
-    s.kt.ensure(ns * 8ull);
+    // the reverse degrees, scores and keys persist between selections (incremental
+    // refresh): they keep their contents when they grow
+    s.rdeg.grow_keep(ns * 4ull, st);
+    s.score.grow_keep(ns * 8ull, st);
+    s.ks.grow_keep(ns * 8ull, st);
+    s.kt.grow_keep(ns * 8ull, st);
     s.chosen.ensure(ns + 16ull);
     s.qtaken.ensure(ns + 16ull);
 }
@@ -448,7 +580,7 @@ uint64_t selection_bound(const Graph& g) {
 void bridges_reserve(Graph& g) {
     Scratch s(g);
     const uint64_t ns = scratch_nodes(g);
-    size_bridge_scratch(s, ns);
+    size_bridge_scratch(s, ns, g.ctx->stream);
     // the rest of a selection on up to ns nodes: per-block label counts, the selected
     // list, the per-component quota keys, the bridge MST over the selected nodes and
     // the selection's sort keys
@@ -468,7 +600,28 @@ void bridges_reserve(Graph& g) {
     s.pcnt.ensure(64);
     g.ctx->scratch[6].ensure(m * 16 + 16);
     g.bridges.grow_keep(md * sizeof(cs_edge), g.ctx->stream);
+    // the incremental hubness state (snapshot, flags, counter), kept when it grows
+    g.hub_prev_ids.grow_keep(ns * g.k * 4ull, g.ctx->stream);
+    g.hub_prev_cnt.grow_keep(ns * 4ull, g.ctx->stream);
+    g.hub_rd_dirty.grow_keep(ns + 16ull, g.ctx->stream);
+    g.hub_list.ensure(ns * 4ull + 16);
+    g.hub_ctr.ensure(64);
+    hub_track(g);
 }
+
+void hub_track(Graph& g) {
+    const uint64_t ns = scratch_nodes(g) + 16;
+    if (g.hub_changed.bytes >= ns && g.hub_changed.p) return;
+    const size_t old = g.hub_changed.p ? g.hub_changed.bytes : 0;
+    g.hub_changed.grow_keep(ns, g.ctx->stream);
+    CSB_CUDA(cudaMemsetAsync(g.hub_changed.as<uint8_t>() + old, 0, g.hub_changed.bytes - old, g.ctx->stream));
+}
+
+/// The incremental hubness refresh runs when at most n / kRefreshShare lists changed
+/// since the last scoring; beyond that a full pass is cheaper (measured: inserts of
+/// 60k-180k rows into 2-3.6M nodes changed enough lists that the refresh rescored
+/// 60-80 % of the nodes and took 0.6-2.0 ms against 0.5-0.85 ms for the full pass).
+constexpr uint64_t kRefreshShare = 16;
 
 /// Events recorded on a stream at stage boundaries; elapsed() gives the
 /// milliseconds between consecutive marks once the last one has completed.
@@ -516,36 +669,101 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     const uint32_t nb = blocks_for(n);
     s.bc.ensure(nb * 4ull + 64);
     s.ncomp.ensure(64);
+    // the two nearest neighbours first (on clustered k-NN graphs they already join most
+    // of each component), every node pointed at its root, then the other list
+    // entries: their finds are one or two loads and most find the endpoints joined
     k_iota_u32<<<blocks_for(n), kThreads, 0, c.stream>>>(s.parent.as<uint32_t>(), n);
-    k_conn_unite<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k,
-                                                            s.parent.as<uint32_t>(), status);
-    count_launch(c, 2);
+    const uint32_t j_first = std::min<uint32_t>(2, k);
+    k_conn_unite<<<blocks_for(static_cast<uint64_t>(n) * j_first), kThreads, 0, c.stream>>>(
+        g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, 0, j_first, s.parent.as<uint32_t>(), status);
+    k_compress<<<blocks_for(n), kThreads, 0, c.stream>>>(s.parent.as<uint32_t>(), n, status);
+    count_launch(c, 3);
+    if (k > j_first) {
+        k_conn_unite<<<blocks_for(static_cast<uint64_t>(n) * (k - j_first)), kThreads, 0, c.stream>>>(
+            g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, j_first, k, s.parent.as<uint32_t>(), status);
+        count_launch(c);
+    }
     launch_labels(c, s.parent.as<uint32_t>(), n, 1, s.lab.as<uint32_t>(), s.bc.as<uint32_t>(),
                   s.ncomp.as<unsigned long long>());
     ev.mark();  // connectivity
     // ---- hubness
-    s.rdeg.ensure(ns * 4ull);
-    s.score.ensure(ns * 8ull);
-    s.ks.ensure(ns * 8ull);
-    s.kt.ensure(ns * 8ull);
-    CSB_CUDA(cudaMemsetAsync(s.rdeg.p, 0, n * 4ull, c.stream));
-    k_rdeg<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, s.rdeg.as<int>());
-    k_score<<<blocks_for(n), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, k,
-                                                      s.rdeg.as<int>(), s.score.as<double>(),
-                                                      s.ks.as<unsigned long long>(), s.kt.as<unsigned long long>());
-    count_launch(c, 2);
+    // the scores persist between selections (incremental refresh), so these buffers
+    // keep their contents when they grow (here, in a reserve, at a capacity step)
+    s.rdeg.grow_keep(ns * 4ull, c.stream);
+    s.score.grow_keep(ns * 8ull, c.stream);
+    s.ks.grow_keep(ns * 8ull, c.stream);
+    s.kt.grow_keep(ns * 8ull, c.stream);
+    g.hub_prev_ids.grow_keep(ns * k * 4ull, c.stream);
+    g.hub_prev_cnt.grow_keep(ns * 4ull, c.stream);
+    g.hub_rd_dirty.grow_keep(ns + 16ull, c.stream);
+    g.hub_list.ensure(ns * 4ull + 16);
+    g.hub_ctr.ensure(64);
+    hub_track(g);
+    // the refresh pays when few lists changed: it rescores the changed nodes and every
+    // node listing one whose reverse degree moved, which after a large insert is most
+    // of the graph, and then a full pass (one streaming pass over the lists for the
+    // reverse degrees, one for the scores) is cheaper.  The changed nodes are counted
+    // first; above n / kRefreshShare the pass is a full one.
+    bool refresh = g.hub_valid && g.hub_n <= n;
+    uint64_t changed_nodes = n;
+    CSB_CUDA(cudaMemsetAsync(g.hub_ctr.p, 0, 16, c.stream));
+    uint32_t* list_cnt = g.hub_ctr.as<uint32_t>() + 2;
+    if (refresh) {
+        k_hub_changed_list<<<blocks_for(n), kThreads, 0, c.stream>>>(n, static_cast<uint32_t>(g.hub_n),
+                                                                    g.hub_changed.as<uint8_t>(),
+                                                                    g.hub_list.as<uint32_t>(), list_cnt);
+        count_launch(c);
+        uint32_t changed = 0;
+        CSB_CUDA(cudaMemcpyAsync(&changed, list_cnt, 4, cudaMemcpyDeviceToHost, c.stream));
+        CSB_CUDA(cudaStreamSynchronize(c.stream));
+        refresh = static_cast<uint64_t>(changed) * kRefreshShare <= n;
+        changed_nodes = changed;
+    }
+    if (refresh) {
+        if (n > g.hub_n) {  // nodes added since: no reverse neighbours yet, no flags
+            CSB_CUDA(cudaMemsetAsync(s.rdeg.as<int>() + g.hub_n, 0, (n - g.hub_n) * 4ull, c.stream));
+            CSB_CUDA(cudaMemsetAsync(g.hub_rd_dirty.as<uint8_t>() + g.hub_n, 0, n - g.hub_n, c.stream));
+        }
+        k_hub_delta<<<static_cast<unsigned>(c.sm_count) * 16u, kThreads, 0, c.stream>>>(
+            g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, static_cast<uint32_t>(g.hub_n),
+            g.hub_list.as<uint32_t>(), list_cnt, g.hub_prev_ids.as<uint32_t>(), g.hub_prev_cnt.as<uint32_t>(),
+            s.rdeg.as<int>(), g.hub_rd_dirty.as<uint8_t>());
+        count_launch(c);
+        k_score_refresh<<<blocks_for(n), kThreads, 0, c.stream>>>(
+            g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, k, static_cast<uint32_t>(g.hub_n),
+            g.hub_changed.as<uint8_t>(), g.hub_rd_dirty.as<uint8_t>(), s.rdeg.as<int>(), s.score.as<double>(),
+            s.ks.as<unsigned long long>(), s.kt.as<unsigned long long>(), g.hub_ctr.as<unsigned long long>());
+        count_launch(c);
+    } else {
+        CSB_CUDA(cudaMemsetAsync(s.rdeg.p, 0, n * 4ull, c.stream));
+        k_rdeg<<<blocks_for(nk), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k,
+                                                          s.rdeg.as<int>());
+        k_score<<<blocks_for(n), kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.counts.as<uint32_t>(), n, k, k,
+                                                          s.rdeg.as<int>(), s.score.as<double>(),
+                                                          s.ks.as<unsigned long long>(), s.kt.as<unsigned long long>());
+        count_launch(c, 2);
+        // the snapshot the next refresh compares against
+        CSB_CUDA(cudaMemcpyAsync(g.hub_prev_ids.p, g.ids.p, nk * 4ull, cudaMemcpyDeviceToDevice, c.stream));
+        CSB_CUDA(cudaMemcpyAsync(g.hub_prev_cnt.p, g.counts.p, n * 4ull, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    CSB_CUDA(cudaMemsetAsync(g.hub_changed.p, 0, n, c.stream));
+    CSB_CUDA(cudaMemsetAsync(g.hub_rd_dirty.p, 0, n, c.stream));
+    g.hub_valid = true;
+    g.hub_n = n;
     check_launch(c, "hubness");
     ev.mark();  // hubness
-    unsigned long long ncomp64 = 0;
+    unsigned long long ncomp64 = 0, rescored = n;
     CSB_CUDA(cudaMemcpyAsync(&ncomp64, s.ncomp.p, 8, cudaMemcpyDeviceToHost, c.stream));
+    if (refresh) CSB_CUDA(cudaMemcpyAsync(&rescored, g.hub_ctr.p, 8, cudaMemcpyDeviceToHost, c.stream));
     int st = 0;
     CSB_CUDA(cudaMemcpyAsync(&st, status, 4, cudaMemcpyDeviceToHost, c.stream));
     CSB_CUDA(cudaStreamSynchronize(c.stream));
     if (st & kStatusUnionLimit) fail(CS_ERR_TIMEOUT, "connectivity: a union retry loop ran out");
     const uint32_t ncomp = static_cast<uint32_t>(ncomp64);
     g.last_ncomp = ncomp;
-    // ---- budget
-    graph_build_edges(g);
+    // ---- budget: the undirected k-NN edge count (the edges themselves are emitted
+    // when a sweep next needs them)
+    graph_count_knn_edges(g);
     ev.mark();  // edge list
     const uint64_t budget = antihub_budget(g.e_knn, g.dim, n);
     // ---- selection: budget lowest under (score, rdeg, id)
@@ -740,6 +958,9 @@ void select_bridges(Graph& g, uint64_t* out_selected, uint64_t* out_bridges, uin
     bs.bridges = missing.size();
     bs.repair = added;
     bs.knn_components = ncomp;
+    bs.hub_refreshed = refresh ? 1u : 0u;
+    bs.rescored = rescored;
+    bs.changed = changed_nodes;
 }
 
 }  // namespace csb

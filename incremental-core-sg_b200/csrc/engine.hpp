@@ -109,6 +109,8 @@ struct Graph {
     // k-NN edges node-major (src/knn_graph.cpp:132-200), then the bridges.
     bool edges_valid = false;
     bool knn_edges_valid = false;  // the k-NN part (first e_knn entries, node_off) is current
+    bool knn_offsets_valid = false;  // node_off, e_knn and the emit mask are current (edges maybe not emitted)
+    DevBuf emask;                    // per node, which list entries emit an undirected edge
     uint64_t e_knn = 0, e_total = 0;
     DevBuf eu, ev, ew;    // SoA u32/u32/f32 [e_total]
     DevBuf node_off;      // u32 [n+1] offsets of each node's emitted edges
@@ -145,12 +147,19 @@ struct Graph {
     uint64_t sweep_barrier_ns = 0, sweep_hold_ns = 0;
 
     ~Graph();
-    void invalidate_edges() { edges_valid = knn_edges_valid = false; }
+    void invalidate_edges() { edges_valid = knn_edges_valid = knn_offsets_valid = false; }
     /// Only the bridges changed: the k-NN part of the edge list stays, and the next
     /// build re-emits the bridge tail alone.
     void invalidate_bridges() { edges_valid = false; }
     // Stages of the last cs_select_bridges.
     cs_bridge_stats last_bridges{};
+    // Incremental hubness (bridges.cu): the lists as of the last scoring (snapshot and
+    // counts), k_merge's flags of nodes whose membership changed since, the flags of
+    // nodes whose reverse degree changed, a counter; valid after a full pass until the
+    // k-NN arrays are replaced.
+    bool hub_valid = false;
+    uint64_t hub_n = 0;  // nodes scored by the last pass
+    DevBuf hub_prev_ids, hub_prev_cnt, hub_changed, hub_rd_dirty, hub_ctr, hub_list;
     void ensure_capacity(uint64_t need, bool keep);
 };
 
@@ -170,6 +179,9 @@ inline uint64_t scratch_scale(const Graph& g, uint64_t count) {
 
 // graph.cu
 void graph_build_edges(Graph& g);  // cached base edge list (no-op when valid)
+/// The undirected k-NN edge count (e_knn) and per-node offsets of the cached edge
+/// list, without emitting the edges (no-op when current).
+void graph_count_knn_edges(Graph& g);
 /// Allocate the cached edge list and its enumeration scratch for scratch_nodes(g)
 /// nodes now.
 void edges_reserve(Graph& g);
@@ -228,6 +240,10 @@ void knn_insert(Graph& g, const float* rows, uint64_t count, uint32_t row_stride
 // bridges.cu
 /// Allocate the selection scratch for scratch_nodes(g) nodes now.
 void bridges_reserve(Graph& g);
+/// The changed-membership flags of the incremental hubness refresh, for
+/// scratch_nodes(g) nodes (contents kept; new entries zero).  The NN-Descent merge
+/// writes them.
+void hub_track(Graph& g);
 /// An upper bound of the selection size on a graph of up to scratch_nodes(g) nodes
 /// whose k-NN graph has at most 4x the last seen component count (+ 64).
 uint64_t selection_bound(const Graph& g);

@@ -217,7 +217,10 @@ uint64_t graph_materialize_edges(Graph& g, uint32_t mpts, bool reweight, DevBuf&
 void edges_reserve(Graph& g) {
     Ctx& c = *g.ctx;
     const uint64_t ns = scratch_nodes(g), words = (g.k + 31) / 32;
-    c.scratch[0].ensure(ns * words * sizeof(uint32_t) + 4);
+    // a mask that grows loses its contents: offsets counted against it are stale
+    const void* mask_before = g.emask.p;
+    g.emask.ensure(ns * words * sizeof(uint32_t) + 4);
+    if (g.emask.p != mask_before) g.invalidate_edges();
     c.scratch[1].ensure((ns + 1) * sizeof(uint32_t));
     // the cached list: at most k edges per node, and the bridges; growing it drops
     // the cached edges, which are enumerated again when next needed
@@ -259,11 +262,59 @@ void graph_build_edges(Graph& g) {
         g.edges_valid = true;
         return;
     }
-    DevBuf core_unused;
-    g.e_total = graph_materialize_edges(g, 0, false, g.eu, g.ev, g.ew, core_unused, c.scratch[0],
-                                        c.scratch[1], g.node_off);
-    g.e_knn = g.e_total - g.nb;
+    // the k-NN edges' per-node offsets (counted by a bridge selection already, or now),
+    // then the edges themselves in the reference order, then the bridges
+    graph_count_knn_edges(g);
+    const uint32_t n = static_cast<uint32_t>(g.n);
+    const uint64_t e_knn = g.e_knn, total = e_knn + g.nb;
+    if (total > 0xFFFFFFFEull) fail(CS_ERR_UNSUPPORTED, "edge count exceeds 32-bit edge indices");
+    const uint64_t room = std::max(scratch_scale(g, e_knn) + g.nb, total);
+    g.eu.ensure(room * sizeof(uint32_t) + 4);
+    g.ev.ensure(room * sizeof(uint32_t) + 4);
+    g.ew.ensure(room * sizeof(float) + 4);
+    const uint32_t words = (g.k + 31) / 32;
+    const unsigned warps_per_block = kThreads / 32;
+    const unsigned nb = std::max(1u, (n + warps_per_block - 1) / warps_per_block);
+    if (n && e_knn) {
+        k_edge_emit<<<nb, kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.dists.as<float>(), n, g.k, words,
+                                                   g.emask.as<uint32_t>(), g.node_off.as<uint32_t>(), nullptr,
+                                                   g.eu.as<uint32_t>(), g.ev.as<uint32_t>(), g.ew.as<float>());
+        count_launch(c);
+    }
+    if (g.nb) {
+        k_bridge_emit<<<blocks_for(g.nb), kThreads, 0, c.stream>>>(
+            g.bridges.as<cs_edge>(), g.nb, nullptr, g.eu.as<uint32_t>() + e_knn, g.ev.as<uint32_t>() + e_knn,
+            g.ew.as<float>() + e_knn);
+        count_launch(c);
+    }
+    check_launch(c, "edge enumeration");
+    g.e_total = total;
     g.edges_valid = g.knn_edges_valid = true;
+}
+
+void graph_count_knn_edges(Graph& g) {
+    if (g.knn_edges_valid || g.knn_offsets_valid) return;
+    Ctx& c = *g.ctx;
+    const uint32_t n = static_cast<uint32_t>(g.n);
+    const uint32_t words = (g.k + 31) / 32;
+    const uint64_t ns = scratch_nodes(g);
+    g.emask.ensure(ns * words * sizeof(uint32_t) + 4);
+    c.scratch[1].ensure((ns + 1) * sizeof(uint32_t));
+    g.node_off.ensure((ns + 1) * sizeof(uint32_t));
+    const unsigned warps_per_block = kThreads / 32;
+    const unsigned nb = std::max(1u, (n + warps_per_block - 1) / warps_per_block);
+    if (n) {
+        k_edge_mask<<<nb, kThreads, 0, c.stream>>>(g.ids.as<uint32_t>(), g.dists.as<float>(), g.counts.as<uint32_t>(),
+                                                   n, g.k, words, g.emask.as<uint32_t>(), c.scratch[1].as<uint32_t>());
+        count_launch(c);
+    }
+    scan_u32(c, c.scratch[1].as<uint32_t>(), g.node_off.as<uint32_t>(), n);
+    uint32_t e_knn = 0;
+    CSB_CUDA(cudaMemcpyAsync(&e_knn, g.node_off.as<uint32_t>() + n, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             c.stream));
+    CSB_CUDA(cudaStreamSynchronize(c.stream));
+    g.e_knn = e_knn;
+    g.knn_offsets_valid = true;
 }
 
 Graph::~Graph() {
@@ -360,7 +411,10 @@ void graph_set_points(Graph& gr, const float* rows, uint64_t n, uint32_t row_str
             count_launch(c);
             check_launch(c, "pad rows");
         }
-        if (!append) g->knn_n = 0;
+        if (!append) {
+            g->knn_n = 0;
+            g->hub_valid = false;  // new k-NN arrays: the next selection is a full one
+        }
         // new nodes start with empty neighbourhoods (KnnGraph::grow)
         const uint64_t from = append ? g->knn_n : 0;
         if (total > from) {
@@ -429,6 +483,7 @@ cs_status cs_graph_set_knn(cs_graph* gp, const uint32_t* ids, const float* dists
         else CSB_CUDA(cudaMemsetAsync(g->flags.p, 0, n * g->k, c.stream));
         copy_h2d(c, g->counts.p, counts, n * sizeof(uint32_t));
         g->knn_n = n;
+        g->hub_valid = false;
         g->invalidate_edges();
     });
 }

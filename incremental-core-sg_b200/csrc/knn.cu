@@ -352,7 +352,7 @@ template <int LI, int I>
 __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, float* __restrict__ rank,
                         uint8_t* __restrict__ flags, uint32_t* __restrict__ counts, float* __restrict__ thr,
                         CandStore cand, uint32_t* __restrict__ rnew_cnt, uint32_t* __restrict__ rold_cnt,
-                        unsigned long long* __restrict__ updates) {
+                        unsigned long long* __restrict__ updates, uint8_t* __restrict__ changed) {
     static_assert(LI + 1 <= I, "merge layout");
     const uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (u >= n) return;
@@ -472,6 +472,9 @@ __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, floa
         rnew_cnt[u] = 0;
         rold_cnt[u] = 0;
         if (inserted && updates) atomicAdd(updates, static_cast<unsigned long long>(inserted));
+        // a newcomer in the list is a change of membership (none got in: the list
+        // holds the same ids); the incremental hubness refresh reads the flag
+        if (inserted) changed[u] = 1;
     }
 }
 
@@ -793,12 +796,12 @@ void launch_merge(Ctx& c, Graph& g, KnnScratch& s, unsigned long long* updates) 
         k_merge<1, 2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
                                                      store_of(s), s.rnew_cnt.as<uint32_t>(),
-                                                     s.rold_cnt.as<uint32_t>(), updates);
+                                                     s.rold_cnt.as<uint32_t>(), updates, g.hub_changed.as<uint8_t>());
     } else {
         k_merge<2, 4><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
                                                      store_of(s), s.rnew_cnt.as<uint32_t>(),
-                                                     s.rold_cnt.as<uint32_t>(), updates);
+                                                     s.rold_cnt.as<uint32_t>(), updates, g.hub_changed.as<uint8_t>());
     }
     count_launch(c);
 }
@@ -826,6 +829,7 @@ struct Descent {
         if (k > 64) fail(CS_ERR_UNSUPPORTED, "NN-Descent: k > 64");
         const uint64_t nk = static_cast<uint64_t>(n) * k;
         size_descent_scratch(s, scratch_nodes(g));
+        hub_track(g);  // k_merge flags the nodes whose membership changes
         d_updates = s.counters.as<unsigned long long>();
         d_evals = d_updates + 1;
         CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
@@ -930,6 +934,7 @@ void knn_descent(Graph& g, uint32_t sample, uint32_t iters, double delta, uint64
     if (out_rounds) *out_rounds = 0;
     if (g.n == 0) return;
     Ctx& c = *g.ctx;
+    g.hub_valid = false;  // a full build: the next bridge selection scores every node
     Descent d(g, sample);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CSB_CUDA(cudaEventCreate(&e0));

@@ -95,3 +95,51 @@ def test_inserts_within_a_reserve_allocate_nothing(gpu_ctx, oracle):
     validate(ids, dists, counts, len(allpts), k)
     br, _, _ = oracle.bridges(pad_rows(allpts), d, ids, dists, counts)
     assert g.missing_edges().tobytes() == br.tobytes()
+
+
+def test_incremental_hubness_matches_full_after_every_batch(gpu_ctx, oracle):
+    """The bridge re-selection after an insert refreshes the hubness incrementally
+    (HubnessIndex::refresh, src/hubness.cpp:523-544) when few lists changed: the
+    reverse-degree deltas of the changed lists, and only the nodes whose score inputs
+    moved rescored; after a large insert a full pass.  After every batch -- small ones
+    that take the refresh, a large one that takes the full pass -- the selection (order
+    included) and the bridges equal a full pass on the same k-NN graph (a fresh graph
+    given the same arrays) and the oracle's bridge computation."""
+    k = 16
+    base, (old, fresh) = workload(seed=53, n=20000, batch=3000)
+    d = base.shape[1]
+    batches = [old[:40], fresh[:60], old[40:70], fresh[60:110], old[100:3100], fresh[200:250]]
+    g = cs.CoreSG(gpu_ctx, d, k)
+    g.build(base)
+    st = g.bridge_stats()
+    assert st["hub_refreshed"] == 0 and st["rescored"] == len(base)
+    pts = base
+    refreshed = 0
+    for b in batches:
+        g.insert(b)
+        pts = np.concatenate([pts, b])
+        n = len(pts)
+        st = g.bridge_stats()
+        # the rule: the refresh when at most n / 16 lists changed
+        assert st["hub_refreshed"] == int(st["changed"] * 16 <= n)
+        if st["hub_refreshed"]:
+            refreshed += 1
+            assert 0 < st["rescored"] < n
+        else:
+            assert st["rescored"] == n
+        ids, dists, flags, counts = g.knn()
+        h = cs.CoreSG(gpu_ctx, d, k)
+        h.set_points(pts)
+        h.set_knn(ids, dists, flags, counts)
+        h.select_bridges()
+        assert h.bridge_stats()["hub_refreshed"] == 0
+        assert np.array_equal(g.selected(), h.selected())
+        assert g.missing_edges().tobytes() == h.missing_edges().tobytes()
+        br, _, _ = oracle.bridges(pad_rows(pts), d, ids, dists, counts)
+        assert g.missing_edges().tobytes() == br.tobytes()
+        h.close()
+    assert refreshed >= 3, "the small batches should have taken the refresh"
+    # replacing the k-NN arrays starts over with a full pass
+    g.set_knn(*g.knn())
+    g.select_bridges()
+    assert g.bridge_stats()["hub_refreshed"] == 0
