@@ -143,6 +143,46 @@ __device__ __forceinline__ void warp_bitonic(unsigned long long (&key)[I], uint3
     }
 }
 
+/// The last pass of warp_bitonic<I> alone: sorts ascending a sequence of 32 * I items
+/// that is already bitonic (ascending, then descending).  log2(32 I) steps instead of
+/// the full sort's log2(32 I) (log2(32 I) + 1) / 2.
+template <int I>
+__device__ __forceinline__ void warp_bitonic_merge(unsigned long long (&key)[I], uint32_t (&pay)[I]) {
+    const unsigned lane = threadIdx.x & 31u;
+    constexpr int N = 32 * I;
+#pragma unroll
+    for (int stride = N / 2; stride > 0; stride >>= 1) {
+        if (stride >= 32) {
+            const int d = stride / 32;
+#pragma unroll
+            for (int i = 0; i < I; ++i) {
+                if (i & d) continue;
+                const int j = i | d;
+                if (key[i] > key[j]) {
+                    const unsigned long long tk = key[i];
+                    key[i] = key[j];
+                    key[j] = tk;
+                    const uint32_t tp = pay[i];
+                    pay[i] = pay[j];
+                    pay[j] = tp;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < I; ++i) {
+                const unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, key[i], stride);
+                const uint32_t op = __shfl_xor_sync(0xFFFFFFFFu, pay[i], stride);
+                const bool lower = (lane & static_cast<unsigned>(stride)) == 0;
+                const bool take_other = lower ? (ok < key[i]) : (ok > key[i]);
+                if (take_other) {
+                    key[i] = ok;
+                    pay[i] = op;
+                }
+            }
+        }
+    }
+}
+
 // ---- small kernels -----------------------------------------------------------------
 
 /// Metric -> rank units for the stored distances (MetricOp::to_rank); +inf stays.
@@ -301,7 +341,37 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
     // Every lane's offer to u1 goes to the same node: one atomicAdd reserves the
     // warp's places in u1's append buffer (the lanes then fill them in lane order)
     // instead of one contended atomic per lane.
+    // The offers of a chunk are written one chunk later: a chunk's places in the
+    // append buffers are reserved with atomics whose results the stores need, and the
+    // next chunk's distances run while those reservations are on their way (written
+    // in the order: this chunk's distances, the previous chunk's stores, this chunk's
+    // reservations, so a reservation's result register is only read a chunk later).
     uint32_t my_evals = 0;
+    bool p1 = false, p2 = false;           // this lane has a pending row / column offer
+    unsigned long long pk1 = 0, pk2 = 0;   // their keys
+    uint32_t pu1 = 0, prank1 = 0, pu2 = 0; // row node and rank in its ballot; column node
+    uint32_t res1 = 0, res2 = 0;           // reservation results (the row's: its leader lane)
+    int pleader = -1;                      // lane holding the pending row reservation (-1: none)
+    auto flush = [&]() {
+        if (pleader >= 0) {  // warp-uniform
+            const uint32_t base = __shfl_sync(0xFFFFFFFFu, res1, pleader);
+            if (p1) {
+                const uint32_t pos = base + prank1;
+                if (pos < kCap) {
+                    cand.buf[static_cast<uint64_t>(pu1) * kCap + pos] = pk1;
+                } else {
+                    offer_table(cand.table + static_cast<uint64_t>(pu1) * kSlots, pk1);
+                }
+            }
+        }
+        if (p2) {
+            if (res2 < kCap) {
+                cand.buf[static_cast<uint64_t>(pu2) * kCap + res2] = pk2;
+            } else {
+                offer_table(cand.table + static_cast<uint64_t>(pu2) * kSlots, pk2);
+            }
+        }
+    };
     for (uint32_t a = 0; a < nN; ++a) {
         const float* ra = s_row + static_cast<size_t>(a) * pitch;
         const uint32_t u1 = s_id[a];
@@ -316,25 +386,25 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
                 ++my_evals;
             }
             const bool to1 = pair && r < ta;
+            const bool to2 = pair && r < s_thr[b];
             const unsigned m1 = __ballot_sync(0xFFFFFFFFu, to1);
-            if (m1) {
-                uint32_t base = 0;
-                const unsigned leader = __ffs(m1) - 1;
-                if (lane == leader) base = atomicAdd(cand.cnt + u1, static_cast<uint32_t>(__popc(m1)));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                if (to1) {
-                    const uint32_t pos = base + __popc(m1 & ((1u << lane) - 1u));
-                    const unsigned long long key = make_key(r, u2);
-                    if (pos < kCap) {
-                        cand.buf[static_cast<uint64_t>(u1) * kCap + pos] = key;
-                    } else {
-                        offer_table(cand.table + static_cast<uint64_t>(u1) * kSlots, key);
-                    }
-                }
-            }
-            if (pair && r < s_thr[b]) offer(cand, u2, make_key(r, u1));
+            flush();
+            // this chunk's reservations: one atomic for the row node (all lanes' offers
+            // to it), one per lane for its column node
+            const int leader = m1 ? __ffs(m1) - 1 : -1;
+            if (static_cast<int>(lane) == leader) res1 = atomicAdd(cand.cnt + u1, static_cast<uint32_t>(__popc(m1)));
+            if (to2) res2 = atomicAdd(cand.cnt + u2, 1u);
+            p1 = to1;
+            p2 = to2;
+            pk1 = make_key(r, u2);
+            pk2 = make_key(r, u1);
+            pu1 = u1;
+            pu2 = u2;
+            prank1 = __popc(m1 & ((1u << lane) - 1u));
+            pleader = leader;
         }
     }
+    flush();
     if (evals) {
         for (int o = 16; o > 0; o >>= 1) my_evals += __shfl_xor_sync(0xFFFFFFFFu, my_evals, o);
         if (lane == 0) atomicAdd(evals, static_cast<unsigned long long>(my_evals));
@@ -588,23 +658,39 @@ __global__ void k_search(const float* __restrict__ pts, uint32_t stride, const u
             const unsigned long long worst = __shfl_sync(0xFFFFFFFFu, key[1], 31);
             ok = ok && ck < worst;
             if (!__any_sync(0xFFFFFFFFu, ok)) continue;
-            for (int s2 = 0; s2 < 32; ++s2) {
+            // a node already in the pool has exactly this key there (the same
+            // distance bits and id): a binary search over the sorted pool (element
+            // e = i * 32 + lane, ascending, empty slots last) finds it
+            {
+                uint32_t lo = 0;
 #pragma unroll
-                for (int i = 0; i < 2; ++i) {
-                    const unsigned long long pk = __shfl_sync(0xFFFFFFFFu, key[i], s2);
-                    if (pk != kNoKey && static_cast<uint32_t>(pk) == nb) ok = false;
+                for (uint32_t half = 32; half > 0; half >>= 1) {
+                    const uint32_t e = lo + half - 1;
+                    const unsigned long long v0 = __shfl_sync(0xFFFFFFFFu, key[0], e & 31u);
+                    const unsigned long long v1 = __shfl_sync(0xFFFFFFFFu, key[1], e & 31u);
+                    if ((e < 32 ? v0 : v1) < ck) lo += half;
                 }
+                const unsigned long long v0 = __shfl_sync(0xFFFFFFFFu, key[0], lo & 31u);
+                const unsigned long long v1 = __shfl_sync(0xFFFFFFFFu, key[1], lo & 31u);
+                if (lo < 64 && (lo < 32 ? v0 : v1) == ck) ok = false;
             }
             {  // forward and reverse entries can name the same node
                 const unsigned same = __match_any_sync(0xFFFFFFFFu, nb);
                 if (static_cast<int>(lane) != __ffs(same) - 1) ok = false;
             }
-            key[2] = ok ? ck : kNoKey;
-            pay[2] = 0;
-            key[3] = kNoKey;
-            pay[3] = 0;
             if (!__any_sync(0xFFFFFFFFu, ok)) continue;
-            warp_bitonic<4>(key, pay);
+            // merge: the candidates sorted (32, one a lane) and placed descending behind
+            // a block of empty slots make the 128 items bitonic; one merge pass sorts them
+            {
+                unsigned long long ckk[1] = {ok ? ck : kNoKey};
+                uint32_t cp[1] = {0};
+                warp_bitonic<1>(ckk, cp);
+                key[2] = kNoKey;
+                pay[2] = 0;
+                key[3] = __shfl_sync(0xFFFFFFFFu, ckk[0], 31u - lane);
+                pay[3] = 0;
+            }
+            warp_bitonic_merge<4>(key, pay);
             key[2] = key[3] = kNoKey;
         }
     }
