@@ -286,3 +286,39 @@ def test_sweep_matches_plain_at_scale(gpu_ctx, shape):
         plain, swept = g.mst(m), g.sweep_fetch(m - 1)
         assert swept.edges.tobytes() == plain.edges.tobytes()
         assert np.array_equal(swept.component, plain.component) and swept.weight == plain.weight
+
+
+def test_k_max_above_32(gpu_ctx, oracle):
+    """k_max = 48: the device build (the 128-element merge network), the bridges, a sweep
+    of mpts 1..48 (two chained passes of 32 and 16 lanes) and the plain path against the
+    oracle, then a small insert whose bridge re-selection takes the incremental hubness
+    refresh with lists longer than 32 (the delta's two halves)."""
+    from coresg_b200.datagen import gaussian_mixture, pad_rows
+    from test_knn_gpu import validate
+
+    pts = gaussian_mixture(4000, 12, 6, (0.2, 1.0), 0.05, seed=91)
+    k, d = 48, 12
+    g = cs.CoreSG(gpu_ctx, d, k)
+    g.build(pts, sample=16, iters=10, seed=42)
+    ids, dists, flags, counts = g.knn()
+    n = len(pts)
+    validate(ids, dists, counts, n, k)
+    br, _, _ = oracle.bridges(pad_rows(pts), d, ids, dists, counts)
+    assert g.missing_edges().tobytes() == br.tobytes()
+    mp = list(range(1, k + 1))
+    res = g.all_msts(mp)
+    for m in (1, 17, 32, 33, 40, 48):
+        e = oracle.edges(m, ids, dists, counts, br)
+        o = oracle.mst(e, n)
+        for r in (res[m - 1], g.mst(m)):
+            assert r.edges.tobytes() == e[o["in_tree"]].tobytes()
+            assert np.array_equal(r.component, o["labels"]) and r.weight == o["weight"]
+    extra = gaussian_mixture(40, d, 6, (0.2, 1.0), 0.0, seed=92)
+    g.insert(extra)
+    allpts = np.concatenate([pts, extra])
+    ids, dists, flags, counts = g.knn()
+    validate(ids, dists, counts, len(allpts), k)
+    st = g.bridge_stats()
+    assert st["hub_refreshed"] == int(st["changed"] * 16 <= len(allpts))
+    br, _, _ = oracle.bridges(pad_rows(allpts), d, ids, dists, counts)
+    assert g.missing_edges().tobytes() == br.tobytes()
