@@ -53,19 +53,15 @@ __device__ __forceinline__ uint32_t slot2(uint32_t id) {
     return a == slot1(id) ? (a ^ 1u) : a;
 }
 
-/// Overflow table: atomicMin into the id's first slot; whichever key loses there
-/// (the offer, or the key it displaced) gets one more atomicMin into its other
-/// slot.  A key equal to the slot's content is already present and stops.
+/// Overflow table: the key is reduced (atomicMin) into both of its id's slots, so it
+/// survives while it is the smallest of either slot.  Neither atomic returns a value,
+/// so an offer never waits on the table (the overflow takes most of the offers of the
+/// first rounds, when the lists are random); a key held by both slots is read twice
+/// and the merge drops the second copy.
 __device__ __forceinline__ void offer_table(unsigned long long* __restrict__ table, unsigned long long key) {
     const uint32_t id = static_cast<uint32_t>(key);
-    const uint32_t s1 = slot1(id);
-    const unsigned long long old = atomicMin(table + s1, key);
-    if (old == key) return;
-    const unsigned long long loser = old < key ? key : old;
-    if (loser == kNoKey) return;
-    const uint32_t lid = static_cast<uint32_t>(loser);
-    const uint32_t alt = slot1(lid) == s1 ? slot2(lid) : slot1(lid);
-    atomicMin(table + alt, loser);
+    atomicMin(table + slot1(id), key);
+    atomicMin(table + slot2(id), key);
 }
 
 /// Offer a packed (rank, id) key to node u: the first kCap offers of a round are
