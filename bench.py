@@ -834,7 +834,9 @@ def main():
     log(f"[rank {rank}] sweep {ms_per_step:.3f} ms/step (kernel {kernel_ms:.3f} ms) wall {wall:.3f}s")
     # per-round profile of the last timed sweep's persistent kernel (cs_sweep_trace)
     trace = [{"phase_a_ms": int(t[0]) / 1e6, "phase_b_ms": int(t[1]) / 1e6, "flatten_ms": int(t[2]) / 1e6,
-              "edges": int(t[3]), "roots": int(t[4]), "full_flatten": int(t[5]), "live_pairs": int(t[6])}
+              "edges": int(t[3]), "roots": int(t[4]), "full_flatten": int(t[5]) & 1,
+              "phase_a_walk": ("edges", "edges + tail table", "tail entries")[min(int(t[5]) >> 1, 2)],
+              "live_pairs": int(t[6])}
              for t in g.sweep_trace()]
 
     # ---- plain per-mpts path on the same graph (one pass over 1..K)

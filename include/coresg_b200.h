@@ -329,8 +329,10 @@ cs_status cs_sweep_fetch_device(cs_graph* g, uint32_t index, cs_edge* d_out_edge
  * Boruvka kernel alone (CUDA events on the context stream), in milliseconds. */
 cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
 /* Per-round profile of the first pass of the last sweep, 7 words per Boruvka round:
- * device ns of phase A (offers), phase B (links) and the forest flatten, edges phase A
- * walked, roots phase B walked, every node flattened (0/1), live (edge, MST) pairs
+ * device ns of phase A (offers), phase B (links) and the forest flatten, entries phase A
+ * walked (edges, or the contracted tail's (MST, component pair) entries), roots phase B
+ * walked, flags (bit 0: every node flattened; bits 1-2: what phase A walked -- 0 the
+ * edges, 1 the edges while filling the tail table, 2 the tail entries), live pairs
  * phase A found.
  * Writes min(rounds, cap_rounds) rows; *out_rounds = rounds (the last round ends after
  * its phase A). */

@@ -58,6 +58,12 @@ constexpr int kThreads = 256;
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
 constexpr int kMaxBlock = 512;
+#ifndef CSB_SWEEP_TAIL_DIV
+#define CSB_SWEEP_TAIL_DIV 4
+#endif
+// the contracted tail starts once a round's root list holds at most n / kTailDiv
+// nodes (0: never)
+constexpr uint32_t kTailDiv = CSB_SWEEP_TAIL_DIV;
 // per round: globaltimer at the round's start, after phase A, after phase B, after
 // the flatten; edges phase A walked; roots phase B walked; live (edge, MST) pairs
 // phase A found; whether every node was flattened
@@ -87,7 +93,12 @@ struct SweepArgs {
     uint32_t* fl;              // [n] frozen root list: roots as of the last full flatten
     const float* core;         // [n][32] core distance of v at mpts[j]
     uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] root-list counts; [4] rounds;
-                               // [5],[6] "some edge offered" flags; [7] frozen-list count
+                               // [5],[6] "some edge offered" flags; [7] frozen-list count;
+                               // [8] tail table overflow; [9],[10] tail entry counts
+    uint32_t tail_roots;       // contract once a round's root list is at most this (0: never)
+    uint32_t tail_cap;         // tail table slots (a power of two); each entry list holds as many
+    ulonglong2* ttab;          // [tail_cap] tail table: (MST, root pair) -> smallest key
+    ulonglong2* tl;            // [2][tail_cap] tail entries: (MST, root pair), key
     unsigned* bar;
     int* status;
     uint64_t limit_ns;
@@ -228,6 +239,203 @@ struct OfferCache {
     }
 };
 
+// ---- the contracted tail --------------------------------------------------------
+// Once a round's root list is short, the live (edge, MST) pairs collapse onto few
+// component pairs.  The table round reduces every live pair's key into a hash table
+// keyed by (MST, smaller root, larger root): of the edges joining two components only
+// the lightest can enter the tree (the others close a cycle with it and tree edges of
+// those components, and are its heaviest edge), so the table's entries carry the rest
+// of the forest.  From the next round on, phase A walks the entries -- one thread per
+// (MST, component pair) -- instead of the edge worklist.
+
+constexpr unsigned long long kTailEmpty = ~0ull;
+constexpr int kTailProbes = 64;      // linear-probe limit; beyond it the table overflows
+constexpr int kTailNodeBits = 27;    // root ids in a tail key: graphs of at most 2^27 nodes
+
+/// Tail key of MST j's component pair {x, y}: j in the top 5 bits, the smaller root in
+/// the next 27, the larger in the low 32.
+__device__ __forceinline__ unsigned long long tail_key(unsigned j, uint32_t x, uint32_t y) {
+    const uint32_t lo = x < y ? x : y, hi = x < y ? y : x;
+    return (static_cast<unsigned long long>(j) << 59) | (static_cast<unsigned long long>(lo) << 32) | hi;
+}
+
+/// Slot of a tail key: the splitmix64 finaliser (Steele, Lea, Flood 2014) of the key.
+__device__ __forceinline__ uint32_t tail_slot(unsigned long long k, uint32_t mask) {
+    k ^= k >> 30;
+    k *= 0xbf58476d1ce4e5b9ull;
+    k ^= k >> 27;
+    k *= 0x94d049bb133111ebull;
+    k ^= k >> 31;
+    return static_cast<uint32_t>(k) & mask;
+}
+
+/// Reduce `key` into the entry of tail key `tk`: linear probing from its slot; a slot
+/// already holding tk takes an atomicMin, an empty one is claimed with atomicCAS.  A
+/// probe sequence longer than kTailProbes sets the overflow flag, and the sweep carries
+/// on over its worklist (written in the table round as in any other).
+__device__ __forceinline__ void tail_insert(const SweepArgs& a, uint32_t mask, unsigned long long tk,
+                                            unsigned long long key) {
+    uint32_t s = tail_slot(tk, mask);
+    for (int p = 0; p < kTailProbes; ++p) {
+        unsigned long long* slot = &a.ttab[s].x;
+        unsigned long long cur = __ldcg(slot);
+        if (cur == kTailEmpty) cur = atomicCAS(slot, kTailEmpty, tk);
+        if (cur == kTailEmpty || cur == tk) {
+            atomicMin(&a.ttab[s].y, key);
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+    a.ctr[8] = 1u;
+}
+
+constexpr int kTailBuf = 160;  // per-warp staging of table inserts: < 32 left + 4 edges x 32 lanes
+
+/// The table round's inserts.  Each lane reduces consecutive live pairs that join the
+/// same two components (edges of one emitter into one neighbouring component) in a
+/// one-entry register cache.  What a lane evicts is staged in its warp's shared-memory
+/// buffer, and after every group of edges the staged entries are inserted 32 at a
+/// time, one per lane, so their table round trips overlap instead of stalling the
+/// walk once per evicting edge.
+struct TailStage {
+    unsigned long long tk = kTailEmpty, key = kNoKey;  // this lane's cache
+    ulonglong2* buf;                                   // the warp's kTailBuf entries
+    uint32_t cnt = 0;                                  // staged entries (warp-uniform)
+    /// Warp-collective: the lanes with `has` reduce (k, v) into their cache.
+    __device__ __forceinline__ void add(bool has, unsigned long long k, unsigned long long v) {
+        const unsigned lane = threadIdx.x & 31u;
+        const bool ev = has && k != tk && tk != kTailEmpty;
+        const unsigned em = __ballot_sync(0xFFFFFFFFu, ev);
+        if (ev) buf[cnt + __popc(em & ((1u << lane) - 1u))] = make_ulonglong2(tk, key);
+        cnt += static_cast<uint32_t>(__popc(em));
+        if (has) {
+            if (k == tk) {
+                key = v < key ? v : key;
+            } else {
+                tk = k;
+                key = v;
+            }
+        }
+    }
+    /// Warp-collective: insert staged entries 32 at a time while at least `keep_below`
+    /// remain (32: leave fewer than 32 staged; 1: insert all).
+    __device__ __forceinline__ void drain(const SweepArgs& a, uint32_t mask, uint32_t keep_below) {
+        const unsigned lane = threadIdx.x & 31u;
+        if (cnt < keep_below) return;
+        __syncwarp();
+        while (cnt >= keep_below && cnt > 0) {
+            const uint32_t m = cnt < 32u ? cnt : 32u;
+            if (lane < m) {
+                const ulonglong2 e = buf[cnt - m + lane];
+                tail_insert(a, mask, e.x, e.y);
+            }
+            cnt -= m;
+        }
+        __syncwarp();
+    }
+    /// Warp-collective: stage every lane's cached entry and insert everything.
+    __device__ __forceinline__ void flush(const SweepArgs& a, uint32_t mask) {
+        const unsigned lane = threadIdx.x & 31u;
+        const bool ev = tk != kTailEmpty;
+        const unsigned em = __ballot_sync(0xFFFFFFFFu, ev);
+        if (ev) buf[cnt + __popc(em & ((1u << lane) - 1u))] = make_ulonglong2(tk, key);
+        cnt += static_cast<uint32_t>(__popc(em));
+        tk = kTailEmpty;
+        key = kNoKey;
+        drain(a, mask, 1u);
+    }
+};
+
+/// Warp-collective append of the entries whose lanes have `keep` set to entry list
+/// `which` (one atomicAdd per warp, lane order).
+__device__ __forceinline__ void tail_append(const SweepArgs& a, int which, bool keep, ulonglong2 e) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned km = __ballot_sync(0xFFFFFFFFu, keep);
+    if (!km) return;
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(a.ctr + 9 + which, static_cast<uint32_t>(__popc(km)));
+    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+    if (keep) a.tl[static_cast<uint64_t>(which) * a.tail_cap + at + __popc(km & ((1u << lane) - 1u))] = e;
+}
+
+/// Phase B of the table round also compacts the table's `slots` slots into entry list
+/// `which` (slots is a power of two, at least 1024, so every warp chunk is full).
+__device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots, int which, uint32_t gw,
+                                             uint32_t nw) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (uint32_t base = gw * 32u; base < slots; base += nw * 32u) {
+        const ulonglong2 e = __ldcg(a.ttab + base + lane);
+        tail_append(a, which, e.x != kTailEmpty, e);
+    }
+}
+
+/// Smallest 64-bit key over the lanes of `grp` (every lane of the group calls it).
+__device__ __forceinline__ unsigned long long group_min_key(unsigned grp, unsigned long long key) {
+    const uint32_t hi = __reduce_min_sync(grp, static_cast<uint32_t>(key >> 32));
+    const uint32_t lo = __reduce_min_sync(grp, static_cast<uint32_t>(key >> 32) == hi ? static_cast<uint32_t>(key)
+                                                                                       : 0xFFFFFFFFu);
+    return (static_cast<unsigned long long>(hi) << 32) | lo;
+}
+
+/// Warp-collective offer of `key` to best[root][j] by the lanes with `has`: the lanes
+/// offering to the same (root, MST) are reduced first and their leader issues one
+/// atomicMin (the few roots of the late rounds take most of the warp's offers).
+__device__ __forceinline__ void offer_grouped(const SweepArgs& a, bool has, uint32_t root, unsigned j,
+                                              unsigned long long key) {
+    const unsigned lane = threadIdx.x & 31u;
+    // roots are below 2^27, so (root << 5 | j) never equals a lane's placeholder
+    const unsigned long long gk = has ? ((static_cast<unsigned long long>(root) << 5) | j) : (kTailEmpty - lane);
+    const unsigned grp = __match_any_sync(0xFFFFFFFFu, gk);
+    const unsigned long long m = group_min_key(grp, key);
+    if (has && lane == static_cast<unsigned>(__ffs(grp) - 1)) offer_min(a, root, j, m);
+}
+
+/// Phase A of a tail round: one thread per entry (MST j, roots x < y as of the round
+/// the entry was last kept, the lightest key between them).  The current roots are
+/// read without writing (the chase from a root of an earlier round through the links
+/// made since: tail rounds do not flatten).  An entry whose roots still differ offers
+/// its key to both and is kept, rewritten with them; entries of a warp that now join
+/// the same two components keep only the lightest.
+__device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw,
+                                           uint32_t& live_pairs) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int par = r & 1;
+    const uint32_t cnt = __ldcg(a.ctr + 9 + par);
+    const ulonglong2* in = a.tl + static_cast<uint64_t>(par) * a.tail_cap;
+    bool offered = false;
+    for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
+        const uint32_t t = base + lane;
+        bool keep = false;
+        ulonglong2 e = make_ulonglong2(kTailEmpty, kNoKey);
+        unsigned j = 0;
+        uint32_t rx = 0, ry = 0;
+        if (t < cnt) {
+            e = __ldcg(in + t);
+            j = static_cast<unsigned>(e.x >> 59);
+            const uint32_t x = static_cast<uint32_t>(e.x >> 32) & ((1u << kTailNodeBits) - 1u);
+            const uint32_t y = static_cast<uint32_t>(e.x);
+            rx = root32(a.parent, x, j, a.n, a.status);
+            ry = root32(a.parent, y, j, a.n, a.status);
+            keep = rx != ry;
+            if (keep) e.x = tail_key(j, rx, ry);
+        }
+        {
+            const unsigned grp = __match_any_sync(0xFFFFFFFFu, keep ? e.x : kTailEmpty - lane);
+            const unsigned long long m = group_min_key(grp, e.y);
+            if (keep) {
+                e.y = m;
+                keep = lane == static_cast<unsigned>(__ffs(grp) - 1);
+            }
+        }
+        offer_grouped(a, keep, rx, j, e.y);
+        offer_grouped(a, keep, ry, j, e.y);
+        live_pairs += keep ? 1u : 0u;
+        offered = offered || keep;
+        tail_append(a, (r + 1) & 1, keep, e);
+    }
+    return offered;
+}
+
 /// Phase A of rounds 0 and 1 for one bridge edge (i, u, v, w), all lanes
 /// (warp-collective).  In round 1 the edge's live lanes are stored and a live edge
 /// is appended to the next worklist.  Returns whether this lane offered.
@@ -355,10 +563,12 @@ __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint3
 /// a later root that phase B's path halving wrote), which is a node of the frozen
 /// root list or a final root, and the flatten after every phase B points each node
 /// of the frozen list at its current root.  Nothing is written back, so the second
-/// loads of a group are issued together after the first ones.
-template <bool kFlat>
+/// loads of a group are issued together after the first ones.  With kTable (the table
+/// round) every live pair's key is also reduced into the tail table (slot mask tmask).
+template <bool kFlat, bool kTable>
 __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, bool act,
-                                         OfferCache& oc, uint32_t& live_pairs) {
+                                         OfferCache& oc, uint32_t& live_pairs, uint32_t tmask,
+                                         ulonglong2* stage) {
     constexpr int G = kFlat ? kWlGroupFlat : kWlGroupHop;
     const unsigned lane = threadIdx.x & 31u;
     const int par = r & 1;
@@ -366,6 +576,9 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
     const uint32_t cnt = __ldcg(a.ctr + par);
     const uint4* in = a.wl + static_cast<uint64_t>(par) * a.E;
     const uint32_t* in_live = a.live + static_cast<uint64_t>(par) * a.E;
+    static_assert(kTailBuf >= 32 + 32 * G, "a group's staged inserts must fit the warp's buffer");
+    TailStage tc;
+    tc.buf = stage + (threadIdx.x >> 5) * kTailBuf;
     for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
         const uint32_t m = min(32u, cnt - base);
         uint4 my_e = make_uint4(0u, 0u, 0u, 0u);
@@ -413,21 +626,25 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
                 const float w = __shfl_sync(0xFFFFFFFFu, my_w, src);
                 const bool lv = ((okm >> x) & 1u) && ru[x] != rv[x];
                 live_pairs += lv ? 1u : 0u;
+                unsigned long long key = kNoKey;
                 if (lv) {
-                    const unsigned long long key = pack_key(max_ref(w, max_ref(cu[x], cv[x])), i);
+                    key = pack_key(max_ref(w, max_ref(cu[x], cv[x])), i);
                     oc.offer(a, lane, ru[x], key);
                     oc.offer(a, lane, rv[x], key);
                     offered = true;
                 }
+                if (kTable) tc.add(lv, tail_key(lane, ru[x], rv[x]), key);
                 if (t + x < m) {  // ballot next to the value it reads
                     const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
                     if (lane == t + x) my_new = L;
                     if (L) pmask |= 1u << (t + x);
                 }
             }
+            if (kTable) tc.drain(a, tmask, 32u);
         }
         chunk_append_edges(a, (r + 1) & 1, pmask, my_e, my_new);
     }
+    if (kTable) tc.flush(a, tmask);
     return offered;
 }
 
@@ -441,22 +658,31 @@ __device__ __forceinline__ void point_at_root(uint32_t* parent, uint32_t c, unsi
     if (f != p) *pc = f;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
+// two blocks of kMaxBlock threads per SM: at most 64 registers a thread
+__global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
+    __shared__ ulonglong2 s_stage[(kMaxBlock / 32) * kTailBuf];  // the table round's insert staging
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     const bool act = lane < a.K;
     bool flat = true;  // parents are the identity at the start
+    // 0: phase A walks the edges; 1: the table round (edges, and the tail table is
+    // filled); 2: phase A walks the tail entries.  Grid-uniform: every change follows
+    // a value read after a grid barrier.
+    int mode = 0;
+    bool tail_ok = a.tail_roots != 0;
+    uint32_t tmask = 0;
     int r = 0;
     for (; r < kMaxRounds; ++r) {
         const int par = r & 1, nxt = (r + 1) & 1;
+        const int rmode = mode;
         unsigned long long* tr = a.trace + static_cast<uint64_t>(r) * kTraceWords;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.ctr[2 + nxt] = 0;  // the root list phase B of this round writes
             a.ctr[5 + nxt] = 0;  // next round's offer flag
             tr[0] = global_ns();  // the other words start zeroed (pre graph)
-            tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + par);
+            tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + (mode == 2 ? 9 + par : par));
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
         }
         OfferCache oc;
@@ -470,9 +696,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                 const bool o = bridge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), r, act, oc);
                 offered = offered || o;
             }
+        } else if (mode == 2) {
+            offered = tail_round(a, r, gw, nw, live_pairs);
+        } else if (mode == 1) {
+            offered = flat ? wl_round<true, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage)
+                           : wl_round<false, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage);
         } else {
-            offered = flat ? wl_round<true>(a, r, gw, nw, act, oc, live_pairs)
-                           : wl_round<false>(a, r, gw, nw, act, oc, live_pairs);
+            offered = flat ? wl_round<true, false>(a, r, gw, nw, act, oc, live_pairs, 0u, s_stage)
+                           : wl_round<false, false>(a, r, gw, nw, act, oc, live_pairs, 0u, s_stage);
         }
         oc.flush(a, lane);
         {
@@ -493,6 +724,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[1] = global_ns();
         if (__ldcg(a.ctr + 5 + par) == 0u) break;
+        if (mode == 1 && __ldcg(a.ctr + 8) != 0u) {
+            // the table overflowed: this round's worklist carries on, no tail
+            mode = 0;
+            tail_ok = false;
+        }
         // ---- phase B: every root that took an offer (all nodes in round 0) links
         // along its best edge; the roots that took one form the next round's list
         // (a root without an offer has no outgoing live edge: its tree is final)
@@ -519,15 +755,21 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                 chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
             }
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[par] = 0;  // this round's worklist, consumed
+        if (mode == 1) tail_compact(a, tmask + 1u, nxt, gw, nw);  // the first tail entries
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.ctr[par] = 0;      // this round's worklist, consumed
+            a.ctr[9 + par] = 0;  // and its tail entries
+        }
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[2] = global_ns();
         // ---- flatten.  Step 1 points at its final root every node of the list whose
         // roots phase B may have linked: in rounds 0 and 1 the list phase B walked
         // (every node with an edge, so that is a full flatten), later the frozen root
         // list (roots as of the last full flatten; it holds every root of this round).
-        // Round 1 freezes round 2's root list.
-        {
+        // Round 1 freezes round 2's root list.  The tail rounds skip it: their lookups
+        // chase from roots without writing (the table round's flatten leaves the first
+        // tail round one load from each root).
+        if (mode != 2) {
             const uint32_t cnt = r == 0 ? a.n : __ldcg(a.ctr + (r == 1 ? 2 + par : 7));
             const uint32_t* lst = r == 1 ? a.rlist + static_cast<uint64_t>(par) * a.n : a.fl;
             for (uint32_t t = gw; t < cnt; t += nw) {
@@ -539,15 +781,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
                 for (uint32_t t = gt; t < nc; t += nt) a.fl[t] = __ldcg(src + t);
                 if (gt == 0) a.ctr[7] = nc;
             }
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
-        if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         // ---- step 2, from round 2 on: every node, when this round's live (edge, MST)
         // pairs say the next round's second root loads would cost more than a pass over
         // the nodes; it freezes the next round's root list.  After step 1 a node's entry
         // is a frozen-list node or a final root, whose entry is its root: two loads.
         const uint64_t pairs = __ldcg(tr + 6);
-        const bool full =
-            r >= 2 && a.flatten_div != 0 && pairs > static_cast<uint64_t>(a.n) * kLanes / a.flatten_div;
+        const bool full = mode == 0 && r >= 2 && a.flatten_div != 0 &&
+                          pairs > static_cast<uint64_t>(a.n) * kLanes / a.flatten_div;
         if (full) {
             for (uint32_t v = gw; v < a.n; v += nw) {
                 if (act) {
@@ -566,9 +808,22 @@ __global__ void __launch_bounds__(kMaxBlock) k_sweep(SweepArgs a) {
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
         flat = r <= 1 || full;
+        if (mode == 1) mode = 2;
+        // ---- arm the table round when the next round's root list is short (the
+        // tail's keys hold root ids below 2^27; the host sets tail_roots only then).
+        // This round's live pairs bound the next round's, so the table gets at least
+        // twice as many slots when the buffer allows.
+        if (mode == 0 && tail_ok && r >= 1 && __ldcg(a.ctr + 2 + nxt) <= a.tail_roots) {
+            uint32_t slots = 1024;
+            while (slots < a.tail_cap && static_cast<uint64_t>(slots) < 2 * pairs) slots <<= 1;
+            tmask = slots - 1u;
+            for (uint32_t t = gt; t < slots; t += nt) a.ttab[t] = make_ulonglong2(kTailEmpty, kNoKey);
+            mode = 1;
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             tr[3] = global_ns();
-            tr[7] = flat ? 1u : 0u;
+            tr[7] = (flat ? 1u : 0u) | (static_cast<unsigned>(rmode) << 1);
         }
     }
     if (r == kMaxRounds) {
@@ -781,11 +1036,12 @@ __global__ void k_tree_weight(const cs_edge* __restrict__ out, uint64_t cap, con
 
 struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
+    uint32_t tail_roots = 0, tail_cap = 0;  // contracted tail: trigger and table slots
     bool labels = false;
     uint64_t limit_ns = 0, hold_ns = 0;  // grid-barrier limit and test hold captured in the graph
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
     DevBuf mpts, parent, best, tree, live, wl, rlist, fl, core, ctr, bar, status, cc, tcnt, rootlab, lab, out, counts, bins,
-        trace;
+        trace, ttab, tl;
     cudaGraphExec_t exec_pre = nullptr, exec_main = nullptr, exec_post = nullptr;
     std::vector<uint32_t> host_mpts;
     const void* key_ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -849,6 +1105,10 @@ SweepArgs args_of(Graph& g, SweepPlan& p) {
     a.status = p.status.as<int>();
     a.limit_ns = p.limit_ns;
     a.hold_ns = p.hold_ns;
+    a.tail_roots = p.tail_roots;
+    a.tail_cap = p.tail_cap;
+    a.ttab = p.ttab.as<ulonglong2>();
+    a.tl = p.tl.as<ulonglong2>();
     return a;
 }
 
@@ -1001,6 +1261,15 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->trace.ensure(kMaxRounds * kTraceWords * 8);
         p->bar.ensure(64);
         p->status.ensure(64);
+        // the contracted tail: a table of min(4 n, |E|) slots rounded up to a power of
+        // two, at least 2^10 and at most 2^24 (256 MB; a fuller table overflows and the
+        // sweep keeps its worklist), and two entry lists as long; graphs of 2^27 nodes
+        // or more keep the edge worklist to the end
+        p->tail_cap = 1024;
+        while (p->tail_cap < std::min<uint64_t>(4 * nc, Ec) && p->tail_cap < (1u << 24)) p->tail_cap <<= 1;
+        p->tail_roots = (kTailDiv != 0 && nc < (1ull << kTailNodeBits)) ? static_cast<uint32_t>(n / kTailDiv) : 0u;
+        p->ttab.ensure(static_cast<uint64_t>(p->tail_cap) * 16);
+        p->tl.ensure(2ull * p->tail_cap * 16);
         p->cc.ensure(static_cast<uint64_t>(K) * p->ncn * 4 + 64);
         p->tcnt.ensure(static_cast<uint64_t>(K) * p->nce * 4 + 64);
         if (labels) {
