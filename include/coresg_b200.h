@@ -344,6 +344,15 @@ cs_status cs_sweep_trace(cs_graph* g, uint64_t* out, uint32_t cap_rounds, uint32
  * block_threads: 128, 256 or 512.  0 picks the value cached by cs_autotune_sweep for
  * this (n, |E|, K, SM count), else the defaults (never, 512). */
 cs_status cs_set_sweep_shape(cs_graph* g, uint32_t flatten_div, uint32_t block_threads);
+/* The sweep's contracted tail: once a Boruvka round's root list holds at most
+ * n / tail_div nodes, the next round reduces the live (edge, MST) pairs into a table of
+ * (MST, root pair) -> lightest key and the rounds after it walk the table's entries
+ * instead of the edges; the trees are the same either way.  tail_div: 0 never,
+ * UINT32_MAX the default (4).  table_slots: a cap on the table's slots, a power of two
+ * in [2^10, 2^24] (0: the default, min(4 n, |E|) rounded up, at most 2^24); a table
+ * that fills past its probe limit leaves the sweep on its edge worklist.  Graphs of
+ * 2^27 nodes or more never take the tail.  Plans are recaptured when these change. */
+cs_status cs_set_sweep_tail(cs_graph* g, uint32_t tail_div, uint32_t table_slots);
 /* Project-written autotuner: times every (block, flatten_div) pair on the resident
  * graph and caches the fastest for later sweeps of this shape. */
 cs_status cs_autotune_sweep(cs_graph* g, const uint32_t* mpts, uint32_t K, uint32_t* out_flatten,

@@ -83,6 +83,7 @@ _SIGS = {
     "cs_sweep_timing": (_i32, [_p, _p, _p]),
     "cs_sweep_trace": (_i32, [_p, _p, _u32, _p]),
     "cs_set_sweep_shape": (_i32, [_p, _u32, _u32]),
+    "cs_set_sweep_tail": (_i32, [_p, _u32, _u32]),
     "cs_autotune_sweep": (_i32, [_p, _p, _u32, _p, _p]),
     "cs_ctx_stream": (_p, [_p]),
     "cs_mst_noalloc": (_i32, [_p, _p, _p, _u64, _u32, _p, _p, _p, _p, _p, _p]),
@@ -502,6 +503,12 @@ class CoreSG:
     def set_sweep_shape(self, flatten=0, block=0):
         """flatten: divisor of the flatten rule (0 auto, 0xFFFFFFFF never); block threads."""
         self.ctx.check(lib().cs_set_sweep_shape(self.h, flatten, block))
+
+    def set_sweep_tail(self, tail_div=0xFFFFFFFF, table_slots=0):
+        """Contracted tail of later sweeps (cs_set_sweep_tail): start it once a round's
+        root list holds at most n / tail_div nodes (0: never; the default 0xFFFFFFFF
+        means 4); table_slots caps the tail table (0: the default)."""
+        self.ctx.check(lib().cs_set_sweep_tail(self.h, tail_div, table_slots))
 
     def autotune(self, mpts_values):
         mp = np.ascontiguousarray(mpts_values, np.uint32)

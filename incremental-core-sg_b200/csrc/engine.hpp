@@ -145,6 +145,8 @@ struct Graph {
     // testing hook (cs_test_sweep_barrier): grid-barrier wait limit of the sweep
     // kernel (0: the default) and a delay block 0 takes before its first barrier
     uint64_t sweep_barrier_ns = 0, sweep_hold_ns = 0;
+    uint32_t sweep_tail_div = 0xFFFFFFFFu;  // contracted tail divisor (0: never; all ones: the default)
+    uint32_t sweep_tail_slots = 0;          // cap on the tail table's slots (0: the default)
 
     ~Graph();
     void invalidate_edges() { edges_valid = knn_edges_valid = knn_offsets_valid = false; }

@@ -58,12 +58,9 @@ constexpr int kThreads = 256;
 constexpr uint64_t kBarrierLimitNs = 2000000000ull;
 constexpr uint32_t kChunkEdges = 256;  // tree compaction: edges per warp chunk
 constexpr int kMaxBlock = 512;
-#ifndef CSB_SWEEP_TAIL_DIV
-#define CSB_SWEEP_TAIL_DIV 4
-#endif
 // the contracted tail starts once a round's root list holds at most n / kTailDiv
-// nodes (0: never)
-constexpr uint32_t kTailDiv = CSB_SWEEP_TAIL_DIV;
+// nodes (cs_set_sweep_tail changes it per graph)
+constexpr uint32_t kTailDiv = 4;
 // per round: globaltimer at the round's start, after phase A, after phase B, after
 // the flatten; edges phase A walked; roots phase B walked; live (edge, MST) pairs
 // phase A found; whether every node was flattened
@@ -358,16 +355,6 @@ __device__ __forceinline__ void tail_append(const SweepArgs& a, int which, bool 
     if (keep) a.tl[static_cast<uint64_t>(which) * a.tail_cap + at + __popc(km & ((1u << lane) - 1u))] = e;
 }
 
-/// Phase B of the table round also compacts the table's `slots` slots into entry list
-/// `which` (slots is a power of two, at least 1024, so every warp chunk is full).
-__device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots, int which, uint32_t gw,
-                                             uint32_t nw) {
-    const unsigned lane = threadIdx.x & 31u;
-    for (uint32_t base = gw * 32u; base < slots; base += nw * 32u) {
-        const ulonglong2 e = __ldcg(a.ttab + base + lane);
-        tail_append(a, which, e.x != kTailEmpty, e);
-    }
-}
 
 /// Smallest 64-bit key over the lanes of `grp` (every lane of the group calls it).
 __device__ __forceinline__ unsigned long long group_min_key(unsigned grp, unsigned long long key) {
@@ -388,6 +375,24 @@ __device__ __forceinline__ void offer_grouped(const SweepArgs& a, bool has, uint
     const unsigned grp = __match_any_sync(0xFFFFFFFFu, gk);
     const unsigned long long m = group_min_key(grp, key);
     if (has && lane == static_cast<unsigned>(__ffs(grp) - 1)) offer_min(a, root, j, m);
+}
+
+/// After the table round's phase A: the table's `slots` slots (a power of two, at
+/// least 1024, so every warp chunk is full) are compacted into entry list `which`, and
+/// every entry offers its key to both of its roots (the roots of this round: the
+/// table's keys were read after the last links).
+__device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots, int which, uint32_t gw,
+                                             uint32_t nw) {
+    for (uint32_t base = gw * 32u; base < slots; base += nw * 32u) {
+        const ulonglong2 e = __ldcg(a.ttab + base + (threadIdx.x & 31u));
+        const bool has = e.x != kTailEmpty;
+        const unsigned j = static_cast<unsigned>(e.x >> 59);
+        const uint32_t x = static_cast<uint32_t>(e.x >> 32) & ((1u << kTailNodeBits) - 1u);
+        const uint32_t y = static_cast<uint32_t>(e.x);
+        offer_grouped(a, has, x, j, e.y);
+        offer_grouped(a, has, y, j, e.y);
+        tail_append(a, which, has, e);
+    }
 }
 
 /// Phase A of a tail round: one thread per entry (MST j, roots x < y as of the round
@@ -564,7 +569,8 @@ __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint3
 /// root list or a final root, and the flatten after every phase B points each node
 /// of the frozen list at its current root.  Nothing is written back, so the second
 /// loads of a group are issued together after the first ones.  With kTable (the table
-/// round) every live pair's key is also reduced into the tail table (slot mask tmask).
+/// round) every live pair's key is reduced into the tail table (slot mask tmask)
+/// instead: no offers and no next worklist, the table's entries make both.
 template <bool kFlat, bool kTable>
 __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, bool act,
                                          OfferCache& oc, uint32_t& live_pairs, uint32_t tmask,
@@ -629,12 +635,14 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
                 unsigned long long key = kNoKey;
                 if (lv) {
                     key = pack_key(max_ref(w, max_ref(cu[x], cv[x])), i);
-                    oc.offer(a, lane, ru[x], key);
-                    oc.offer(a, lane, rv[x], key);
+                    if (!kTable) {
+                        oc.offer(a, lane, ru[x], key);
+                        oc.offer(a, lane, rv[x], key);
+                    }
                     offered = true;
                 }
                 if (kTable) tc.add(lv, tail_key(lane, ru[x], rv[x]), key);
-                if (t + x < m) {  // ballot next to the value it reads
+                if (!kTable && t + x < m) {  // ballot next to the value it reads
                     const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
                     if (lane == t + x) my_new = L;
                     if (L) pmask |= 1u << (t + x);
@@ -642,7 +650,7 @@ __device__ __forceinline__ bool wl_round(const SweepArgs& a, int r, uint32_t gw,
             }
             if (kTable) tc.drain(a, tmask, 32u);
         }
-        chunk_append_edges(a, (r + 1) & 1, pmask, my_e, my_new);
+        if (!kTable) chunk_append_edges(a, (r + 1) & 1, pmask, my_e, my_new);
     }
     if (kTable) tc.flush(a, tmask);
     return offered;
@@ -667,9 +675,9 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
     const bool act = lane < a.K;
     bool flat = true;  // parents are the identity at the start
-    // 0: phase A walks the edges; 1: the table round (edges, and the tail table is
-    // filled); 2: phase A walks the tail entries.  Grid-uniform: every change follows
-    // a value read after a grid barrier.
+    // 0: phase A walks the edges; 1: the table round (phase A walks the edges into the
+    // tail table, whose entries then make the offers); 2: phase A walks the tail
+    // entries.  Grid-uniform: every change follows a value read after a grid barrier.
     int mode = 0;
     bool tail_ok = a.tail_roots != 0;
     uint32_t tmask = 0;
@@ -684,6 +692,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
             tr[0] = global_ns();  // the other words start zeroed (pre graph)
             tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + (mode == 2 ? 9 + par : par));
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
+            tr[7] = static_cast<unsigned>(mode) << 1;  // the flatten bit joins at the round's end
         }
         OfferCache oc;
         bool offered = false;
@@ -724,10 +733,25 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) tr[1] = global_ns();
         if (__ldcg(a.ctr + 5 + par) == 0u) break;
-        if (mode == 1 && __ldcg(a.ctr + 8) != 0u) {
-            // the table overflowed: this round's worklist carries on, no tail
-            mode = 0;
-            tail_ok = false;
+        if (mode == 1) {
+            if (__ldcg(a.ctr + 8) != 0u) {
+                // the table overflowed: phase A again over the same worklist, with its
+                // offers and the next worklist; no tail
+                mode = 0;
+                tail_ok = false;
+                uint32_t again = 0;
+                if (flat) {
+                    wl_round<true, false>(a, r, gw, nw, act, oc, again, 0u, s_stage);
+                } else {
+                    wl_round<false, false>(a, r, gw, nw, act, oc, again, 0u, s_stage);
+                }
+                oc.flush(a, lane);
+            } else {
+                // the table's entries become the first tail list, and each offers its
+                // key to both of its roots
+                tail_compact(a, tmask + 1u, nxt, gw, nw);
+            }
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
         // ---- phase B: every root that took an offer (all nodes in round 0) links
         // along its best edge; the roots that took one form the next round's list
@@ -755,7 +779,6 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
             }
         }
-        if (mode == 1) tail_compact(a, tmask + 1u, nxt, gw, nw);  // the first tail entries
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.ctr[par] = 0;      // this round's worklist, consumed
             a.ctr[9 + par] = 0;  // and its tail entries
@@ -1037,6 +1060,7 @@ __global__ void k_tree_weight(const cs_edge* __restrict__ out, uint64_t cap, con
 struct SweepPlan {
     uint32_t n = 0, E = 0, e_knn = 0, K = 0, block = 0, grid = 0, flatten_div = 4;
     uint32_t tail_roots = 0, tail_cap = 0;  // contracted tail: trigger and table slots
+    uint32_t tail_div = 0, tail_slots = 0;  // the graph's knobs they were made from
     bool labels = false;
     uint64_t limit_ns = 0, hold_ns = 0;  // grid-barrier limit and test hold captured in the graph
     uint32_t ncn = 0, nce = 0;  // node chunks, edge chunks
@@ -1265,9 +1289,13 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         // two, at least 2^10 and at most 2^24 (256 MB; a fuller table overflows and the
         // sweep keeps its worklist), and two entry lists as long; graphs of 2^27 nodes
         // or more keep the edge worklist to the end
+        p->tail_div = g.sweep_tail_div;
+        p->tail_slots = g.sweep_tail_slots;
+        const uint32_t tdiv = g.sweep_tail_div == 0xFFFFFFFFu ? kTailDiv : g.sweep_tail_div;
+        const uint32_t tmax = g.sweep_tail_slots ? g.sweep_tail_slots : (1u << 24);
         p->tail_cap = 1024;
-        while (p->tail_cap < std::min<uint64_t>(4 * nc, Ec) && p->tail_cap < (1u << 24)) p->tail_cap <<= 1;
-        p->tail_roots = (kTailDiv != 0 && nc < (1ull << kTailNodeBits)) ? static_cast<uint32_t>(n / kTailDiv) : 0u;
+        while (p->tail_cap < std::min<uint64_t>(4 * nc, Ec) && p->tail_cap < tmax) p->tail_cap <<= 1;
+        p->tail_roots = (tdiv != 0 && nc < (1ull << kTailNodeBits)) ? static_cast<uint32_t>(n / tdiv) : 0u;
         p->ttab.ensure(static_cast<uint64_t>(p->tail_cap) * 16);
         p->tl.ensure(2ull * p->tail_cap * 16);
         p->cc.ensure(static_cast<uint64_t>(K) * p->ncn * 4 + 64);
@@ -1335,6 +1363,7 @@ bool plan_matches(const SweepPlan* p, const Graph& g, uint32_t K, uint32_t block
     return p && p->n == g.n && p->E == g.e_total && p->e_knn == g.e_knn && p->K == K && p->block == block &&
            p->flatten_div == fdiv && p->labels == labels &&
            p->limit_ns == (g.sweep_barrier_ns ? g.sweep_barrier_ns : kBarrierLimitNs) && p->hold_ns == g.sweep_hold_ns &&
+           p->tail_div == g.sweep_tail_div && p->tail_slots == g.sweep_tail_slots &&
            p->key_ptrs[0] == g.eu.p && p->key_ptrs[1] == g.ev.p &&
            p->key_ptrs[2] == g.ew.p && p->key_ptrs[3] == g.dists.p && p->key_ptrs[4] == g.counts.p &&
            p->key_ptrs[5] == g.node_off.p;
@@ -1548,7 +1577,7 @@ cs_status cs_sweep_trace(cs_graph* gp, uint64_t* out, uint32_t cap_rounds, uint3
             o[2] = (!last && x[3] > x[2]) ? x[3] - x[2] : 0;           // flatten
             o[3] = x[4];
             o[4] = x[5];
-            o[5] = last ? 0 : x[7];
+            o[5] = last ? (x[7] & ~1ull) : x[7];
             o[6] = x[6];
         }
         if (out_rounds) *out_rounds = rounds;
@@ -1571,6 +1600,17 @@ cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t flatten_div, uint32_t block_
                     "cs_set_sweep_shape: block must be 128, 256 or 512");
         g->sweep_block = block_threads;
         g->sweep_flatten = flatten_div == 0 ? kFlattenAuto : (flatten_div == 0xFFFFFFFFu ? 0 : flatten_div);
+    });
+}
+
+cs_status cs_set_sweep_tail(cs_graph* gp, uint32_t tail_div, uint32_t table_slots) {
+    Graph* g = reinterpret_cast<Graph*>(gp);
+    return guarded(g ? g->ctx : nullptr, [&] {
+        CSB_REQUIRE(table_slots == 0 || (table_slots >= 1024 && table_slots <= (1u << 24) &&
+                                         (table_slots & (table_slots - 1)) == 0),
+                    "cs_set_sweep_tail: table_slots must be 0 or a power of two in [2^10, 2^24]");
+        g->sweep_tail_div = tail_div;
+        g->sweep_tail_slots = table_slots;
     });
 }
 
