@@ -343,16 +343,30 @@ struct TailStage {
     }
 };
 
-/// Warp-collective append of the entries whose lanes have `keep` set to entry list
-/// `which` (one atomicAdd per warp, lane order).
-__device__ __forceinline__ void tail_append(const SweepArgs& a, int which, bool keep, ulonglong2 e) {
-    const unsigned lane = threadIdx.x & 31u;
+/// Block-collective append of the entries whose threads have `keep` set to entry list
+/// `which`: the warps' counts are scanned in shared memory and one atomicAdd per block
+/// reserves them.  Every thread of the block calls it the same number of times;
+/// `scan` holds kMaxBlock / 32 + 1 words.
+__device__ __forceinline__ void tail_append(const SweepArgs& a, int which, bool keep, ulonglong2 e,
+                                            uint32_t* scan) {
+    const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const unsigned km = __ballot_sync(0xFFFFFFFFu, keep);
-    if (!km) return;
-    uint32_t at = 0;
-    if (lane == 0) at = atomicAdd(a.ctr + 9 + which, static_cast<uint32_t>(__popc(km)));
-    at = __shfl_sync(0xFFFFFFFFu, at, 0);
-    if (keep) a.tl[static_cast<uint64_t>(which) * a.tail_cap + at + __popc(km & ((1u << lane) - 1u))] = e;
+    if (lane == 0) scan[w] = static_cast<uint32_t>(__popc(km));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (unsigned i = 0; i < (blockDim.x >> 5); ++i) {
+            const uint32_t c = scan[i];
+            scan[i] = tot;
+            tot += c;
+        }
+        scan[kMaxBlock / 32] = tot ? atomicAdd(a.ctr + 9 + which, tot) : 0u;
+    }
+    __syncthreads();
+    if (keep)
+        a.tl[static_cast<uint64_t>(which) * a.tail_cap + scan[kMaxBlock / 32] + scan[w] +
+             __popc(km & ((1u << lane) - 1u))] = e;
+    __syncthreads();  // the scan words are reused by the next call
 }
 
 
@@ -381,17 +395,18 @@ __device__ __forceinline__ void offer_grouped(const SweepArgs& a, bool has, uint
 /// least 1024, so every warp chunk is full) are compacted into entry list `which`, and
 /// every entry offers its key to both of its roots (the roots of this round: the
 /// table's keys were read after the last links).
-__device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots, int which, uint32_t gw,
-                                             uint32_t nw) {
-    for (uint32_t base = gw * 32u; base < slots; base += nw * 32u) {
-        const ulonglong2 e = __ldcg(a.ttab + base + (threadIdx.x & 31u));
+__device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots, int which, uint32_t* scan) {
+    // block-uniform trip count: slots and the grid's thread count are multiples of the
+    // block size (powers of two of at least 1024 over 128, 256 or 512)
+    for (uint32_t base = blockIdx.x * blockDim.x; base < slots; base += gridDim.x * blockDim.x) {
+        const ulonglong2 e = __ldcg(a.ttab + base + threadIdx.x);
         const bool has = e.x != kTailEmpty;
         const unsigned j = static_cast<unsigned>(e.x >> 59);
         const uint32_t x = static_cast<uint32_t>(e.x >> 32) & ((1u << kTailNodeBits) - 1u);
         const uint32_t y = static_cast<uint32_t>(e.x);
         offer_grouped(a, has, x, j, e.y);
         offer_grouped(a, has, y, j, e.y);
-        tail_append(a, which, has, e);
+        tail_append(a, which, has, e, scan);
     }
 }
 
@@ -401,15 +416,15 @@ __device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots,
 /// made since: tail rounds do not flatten).  An entry whose roots still differ offers
 /// its key to both and is kept, rewritten with them; entries of a warp that now join
 /// the same two components keep only the lightest.
-__device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw,
-                                           uint32_t& live_pairs) {
+__device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t& live_pairs, uint32_t* scan) {
     const unsigned lane = threadIdx.x & 31u;
     const int par = r & 1;
     const uint32_t cnt = __ldcg(a.ctr + 9 + par);
     const ulonglong2* in = a.tl + static_cast<uint64_t>(par) * a.tail_cap;
     bool offered = false;
-    for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
-        const uint32_t t = base + lane;
+    // block-uniform trip count (tail_append synchronises the block)
+    for (uint32_t base = blockIdx.x * blockDim.x; base < cnt; base += gridDim.x * blockDim.x) {
+        const uint32_t t = base + threadIdx.x;
         bool keep = false;
         ulonglong2 e = make_ulonglong2(kTailEmpty, kNoKey);
         unsigned j = 0;
@@ -436,7 +451,7 @@ __device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t g
         offer_grouped(a, keep, ry, j, e.y);
         live_pairs += keep ? 1u : 0u;
         offered = offered || keep;
-        tail_append(a, (r + 1) & 1, keep, e);
+        tail_append(a, (r + 1) & 1, keep, e, scan);
     }
     return offered;
 }
@@ -669,6 +684,7 @@ __device__ __forceinline__ void point_at_root(uint32_t* parent, uint32_t c, unsi
 // two blocks of kMaxBlock threads per SM: at most 64 registers a thread
 __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
     __shared__ ulonglong2 s_stage[(kMaxBlock / 32) * kTailBuf];  // the table round's insert staging
+    __shared__ uint32_t s_scan[kMaxBlock / 32 + 1];               // the tail lists' block appends
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
@@ -706,7 +722,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 offered = offered || o;
             }
         } else if (mode == 2) {
-            offered = tail_round(a, r, gw, nw, live_pairs);
+            offered = tail_round(a, r, live_pairs, s_scan);
         } else if (mode == 1) {
             offered = flat ? wl_round<true, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage)
                            : wl_round<false, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage);
@@ -749,7 +765,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
             } else {
                 // the table's entries become the first tail list, and each offers its
                 // key to both of its roots
-                tail_compact(a, tmask + 1u, nxt, gw, nw);
+                tail_compact(a, tmask + 1u, nxt, s_scan);
             }
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
