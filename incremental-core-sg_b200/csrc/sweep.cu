@@ -186,7 +186,7 @@ __device__ __forceinline__ void chunk_append_edges(const SweepArgs& a, int which
     }
 }
 
-constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0, 1)
+constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0-2)
 constexpr int kWlGroupFlat = 4;   // worklist edges in flight per warp: one root load per endpoint,
 constexpr int kWlGroupHop = 4;    // or two
 
@@ -456,28 +456,38 @@ __device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t& 
     return offered;
 }
 
-/// Phase A of rounds 0 and 1 for one bridge edge (i, u, v, w), all lanes
-/// (warp-collective).  In round 1 the edge's live lanes are stored and a live edge
-/// is appended to the next worklist.  Returns whether this lane offered.
+/// Phase A of rounds 0-2 for one bridge edge (i, u, v, w), all lanes (warp-collective;
+/// from round 1 on every node holds its root).  kList: a live edge is appended with
+/// its live lanes to worklist `which`; kTable: the live lanes' keys go to the tail
+/// table instead of the offers.  Returns whether this lane found the edge live.
+template <bool kList, bool kTable>
 __device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uint32_t u, uint32_t v, float w, int r,
-                                             bool act, OfferCache& oc) {
+                                             bool act, OfferCache& oc, TailStage& ts, uint32_t tmask, int which) {
     const unsigned lane = threadIdx.x & 31u;
     bool live = false;
+    uint32_t ru = 0, rv = 0;
+    unsigned long long key = kNoKey;
     if (act && u < a.n && v < a.n) {
         const float cu = __ldg(a.core + static_cast<uint64_t>(u) * kLanes + lane);
         const float cv = __ldg(a.core + static_cast<uint64_t>(v) * kLanes + lane);
-        const uint32_t ru = root01(a, u, lane, r), rv = root01(a, v, lane, r);
+        ru = root01(a, u, lane, r);
+        rv = root01(a, v, lane, r);
         live = ru != rv;
         if (live) {
-            const unsigned long long key = pack_key(max_ref(w, max_ref(cu, cv)), i);
-            oc.offer(a, lane, ru, key);
-            oc.offer(a, lane, rv, key);
+            key = pack_key(max_ref(w, max_ref(cu, cv)), i);
+            if (!kTable) {
+                oc.offer(a, lane, ru, key);
+                oc.offer(a, lane, rv, key);
+            }
         }
     }
-    if (r == 1) {
+    if (kTable) {
+        ts.add(live, tail_key(lane, ru, rv), key);
+        ts.drain(a, tmask, 32u);
+    }
+    if (kList) {
         const unsigned L = __ballot_sync(0xFFFFFFFFu, live);
         if (L && lane == 0) {
-            const int which = (r + 1) & 1;
             const uint32_t at = atomicAdd(a.ctr + which, 1u);
             a.wl[static_cast<uint64_t>(which) * a.E + at] = make_uint4(i, u, v, __float_as_uint(w));
             a.live[static_cast<uint64_t>(which) * a.E + at] = L;
@@ -486,16 +496,17 @@ __device__ __forceinline__ bool bridge_lanes(const SweepArgs& a, uint32_t i, uin
     return live;
 }
 
-/// Rounds 0 and 1, one chunk of node p's emitted segment (m <= 32 edges b, b+1, ...;
-/// lane t holds edge b+t's other endpoint and base weight).  kSegGroup edges' core
-/// and root loads are issued together; every live edge's key is folded into p's
-/// minimum `seg` (offered once per node by the caller) and offered to the other
-/// endpoint's root.  Round 1 stores the edges' live lanes
-/// and returns the bits of the edges that stay live.
-template <int R>
+/// Rounds 0-2, one chunk of node p's emitted segment (m <= 32 edges b, b+1, ...; lane
+/// t holds edge b+t's other endpoint and base weight).  kSegGroup edges' core and root
+/// loads are issued together.  Offering rounds fold every live edge's key into p's
+/// minimum `seg` (offered once per node by the caller) and offer it to the other
+/// endpoint's root; the table round (kTable) puts the keys in the tail table instead.
+/// kList stores the edges' live lanes and returns the bits of the edges that stay live.
+template <int R, bool kList, bool kTable>
 __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, float cp, bool act, uint32_t m,
                                               uint32_t b, uint32_t my_q, float my_w, unsigned long long& seg,
-                                              OfferCache& oc, uint32_t& live_pairs, uint32_t& my_live) {
+                                              OfferCache& oc, TailStage& ts, uint32_t tmask, uint32_t& live_pairs,
+                                              uint32_t& my_live) {
     const unsigned lane = threadIdx.x & 31u;
     uint32_t pmask = 0;
     for (uint32_t t = 0; t < m; t += kSegGroup) {
@@ -510,39 +521,52 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
         }
 #pragma unroll
         for (int x = 0; x < kSegGroup; ++x) {
-            const uint32_t q = __shfl_sync(0xFFFFFFFFu, my_q, (t + x) & 31u);
             const float w = __shfl_sync(0xFFFFFFFFu, my_w, (t + x) & 31u);
             const bool lv = act && t + x < m && rp != rq[x];
             live_pairs += lv ? 1u : 0u;
+            unsigned long long key = kNoKey;
             if (lv) {
-                const unsigned long long key = pack_key(max_ref(w, max_ref(cp, cq[x])), b + t + x);
-                seg = key < seg ? key : seg;
-                // round 0: every receiver is its own root and differs edge to edge, so
-                // the cache would only delay the atomic; from round 1 on it merges offers
-                if (R == 0) {
-                    offer_min(a, rq[x], lane, key);
+                key = pack_key(max_ref(w, max_ref(cp, cq[x])), b + t + x);
+                if (!kTable) {
+                    seg = key < seg ? key : seg;
+                    // round 0: every receiver is its own root and differs edge to edge,
+                    // so the cache would only delay the atomic; later it merges offers
+                    if (R == 0) {
+                        offer_min(a, rq[x], lane, key);
+                    } else {
+                        oc.offer(a, lane, rq[x], key);
+                    }
                 } else {
-                    oc.offer(a, lane, rq[x], key);
+                    seg = 0;  // marks that p had a live pair
                 }
             }
-            // round 1 records the live lanes (the lane holding the edge keeps them);
-            // the ballot is taken next to its value
-            if (R == 1 && t + x < m) {
+            if (kTable) {
+                ts.add(lv, tail_key(lane, rp, rq[x]), key);
+                if (x == kSegGroup / 2 - 1) ts.drain(a, tmask, 32u);  // the buffer holds 4 edges' evictions
+            }
+            // kList records the live lanes (the lane holding the edge keeps them); the
+            // ballot is taken next to its value
+            if (kList && t + x < m) {
                 const unsigned L = __ballot_sync(0xFFFFFFFFu, lv);
                 if (lane == t + x) my_live = L;
                 if (L) pmask |= 1u << (t + x);
             }
         }
+        if (kTable) ts.drain(a, tmask, 32u);
     }
     return pmask;
 }
 
-/// Rounds 0 and 1: the k-NN edges node by node over the emitted segments (32 edges
-/// of a segment loaded at once); the emitter's offers are reduced in registers and
-/// issued once.  Round 1 also builds round 2's worklist.
-template <int R>
+/// Rounds 0-2: the k-NN edges node by node over the emitted segments (32 edges of a
+/// segment loaded at once); the emitter's offers are reduced in registers and issued
+/// once.  R = 0: every node is its own root; R = 1: every node holds its root (rounds 1
+/// and 2: rounds 0 and 1 flatten every node).  kList builds worklist `which`; kTable
+/// fills the tail table (round 2 as the table round).
+template <int R, bool kList, bool kTable>
 __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint32_t nw, bool act, OfferCache& oc,
-                                          uint32_t& live_pairs) {
+                                          TailStage& ts, uint32_t tmask, int which, uint32_t& live_pairs) {
+    static_assert(kTailBuf >= 32 + 32 * (kSegGroup - kSegGroup / 2) && kTailBuf >= 32 + 32 * (kSegGroup / 2),
+                  "half a group's staged inserts must fit the warp's buffer");
     const unsigned lane = threadIdx.x & 31u;
     bool offered = false;
     for (uint32_t p = gw; p < a.n; p += nw) {
@@ -561,16 +585,31 @@ __device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint3
                 my_q = my_x == p ? my_y : my_x;
                 my_w = __ldg(a.ew + b + lane);
             }
-            const uint32_t pmask = seg_chunk<R>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, live_pairs, my_live);
-            if (R == 1)
-                chunk_append_edges(a, (R + 1) & 1, pmask, make_uint4(b + lane, my_x, my_y, __float_as_uint(my_w)),
-                                   my_live);
+            const uint32_t pmask =
+                seg_chunk<R, kList, kTable>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, ts, tmask, live_pairs, my_live);
+            if (kList)
+                chunk_append_edges(a, which, pmask, make_uint4(b + lane, my_x, my_y, __float_as_uint(my_w)), my_live);
         }
         if (seg != kNoKey) {
-            offer_min(a, rp, lane, seg);
+            if (!kTable) offer_min(a, rp, lane, seg);
             offered = true;
         }
     }
+    return offered;
+}
+
+/// Phase A of rounds 0-2: the emitted segments, then the bridges one warp per edge.
+template <int R, bool kList, bool kTable>
+__device__ __forceinline__ bool seg_phase(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, bool act,
+                                          OfferCache& oc, TailStage& ts, uint32_t tmask, uint32_t& live_pairs) {
+    const int which = (r + 1) & 1;
+    bool offered = seg_round<R, kList, kTable>(a, gw, nw, act, oc, ts, tmask, which, live_pairs);
+    for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
+        const bool o = bridge_lanes<kList, kTable>(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), r, act, oc,
+                                                   ts, tmask, which);
+        offered = offered || o;
+    }
+    if (kTable) ts.flush(a, tmask);
     return offered;
 }
 
@@ -706,7 +745,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
             a.ctr[2 + nxt] = 0;  // the root list phase B of this round writes
             a.ctr[5 + nxt] = 0;  // next round's offer flag
             tr[0] = global_ns();  // the other words start zeroed (pre graph)
-            tr[4] = r <= 1 ? a.E : __ldcg(a.ctr + (mode == 2 ? 9 + par : par));
+            tr[4] = r <= 2 ? a.E : __ldcg(a.ctr + (mode == 2 ? 9 + par : par));
             tr[5] = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
             tr[7] = static_cast<unsigned>(mode) << 1;  // the flatten bit joins at the round's end
         }
@@ -714,13 +753,16 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
         bool offered = false;
         uint32_t live_pairs = 0;
         // ---- phase A
-        if (r <= 1) {
-            offered = r == 0 ? seg_round<0>(a, gw, nw, act, oc, live_pairs) : seg_round<1>(a, gw, nw, act, oc, live_pairs);
-            // bridges: one warp per edge
-            for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
-                const bool o = bridge_lanes(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), r, act, oc);
-                offered = offered || o;
-            }
+        TailStage ts;
+        ts.buf = s_stage + (threadIdx.x >> 5) * kTailBuf;
+        if (r == 0) {
+            offered = seg_phase<0, false, false>(a, r, gw, nw, act, oc, ts, 0u, live_pairs);
+        } else if (r == 1) {
+            offered = seg_phase<1, false, false>(a, r, gw, nw, act, oc, ts, 0u, live_pairs);
+        } else if (r == 2 && mode == 1) {
+            offered = seg_phase<1, false, true>(a, r, gw, nw, act, oc, ts, tmask, live_pairs);
+        } else if (r == 2) {
+            offered = seg_phase<1, true, false>(a, r, gw, nw, act, oc, ts, 0u, live_pairs);
         } else if (mode == 2) {
             offered = tail_round(a, r, live_pairs, s_scan);
         } else if (mode == 1) {
@@ -756,7 +798,9 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 mode = 0;
                 tail_ok = false;
                 uint32_t again = 0;
-                if (flat) {
+                if (r == 2) {
+                    seg_phase<1, true, false>(a, r, gw, nw, act, oc, ts, 0u, again);
+                } else if (flat) {
                     wl_round<true, false>(a, r, gw, nw, act, oc, again, 0u, s_stage);
                 } else {
                     wl_round<false, false>(a, r, gw, nw, act, oc, again, 0u, s_stage);
