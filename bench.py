@@ -17,8 +17,9 @@ Reported (one JSON line from rank 0):
              device allocations included); rebuild_s the same build again on it
   e2e        the same metric through the C ABI with host buffers: the CORE-SG arrays
              copied host->device and all K trees + labels copied back, every step;
-             two graphs in flight on their own contexts, so one step's copies overlap
-             the other's sweep (e2e.serial: one graph, steps back to back)
+             three graphs in flight on their own contexts (--e2e-inflight), so one
+             step's copies overlap another's sweep (e2e.serial: one graph, steps back
+             to back)
   roofline   the persistent Boruvka kernel against the measured HBM copy bandwidth
   cpu_baseline  the reference CPU extract (built from its sources) on the same
              CORE-SG, a bounded sample of mpts values, all host threads
@@ -744,7 +745,7 @@ def main():
     ap.add_argument("--workload", default="blobs1m_d16")
     ap.add_argument("--n", type=int, default=None, help="override the workload's point count")
     ap.add_argument("--e2e-steps", type=int, default=10, help="e2e steps per graph in flight (0: skip)")
-    ap.add_argument("--e2e-inflight", type=int, default=2, help="e2e graphs in flight, each on its own context")
+    ap.add_argument("--e2e-inflight", type=int, default=3, help="e2e graphs in flight, each on its own context")
     ap.add_argument("--clocks-dir", default=None, help="folder for the raw nvidia-smi samples (default: a temp folder)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")

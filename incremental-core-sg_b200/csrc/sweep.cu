@@ -91,7 +91,9 @@ struct SweepArgs {
     const float* core;         // [n][32] core distance of v at mpts[j]
     uint32_t* ctr;             // [0],[1] worklist counts; [2],[3] root-list counts; [4] rounds;
                                // [5],[6] "some edge offered" flags; [7] frozen-list count;
-                               // [8] tail table overflow; [9],[10] tail entry counts
+                               // [8] tail table overflow; [9],[10] tail entry counts;
+                               // [11],[12] segment-walk node counters; [13],[14] phase B
+                               // root counters
     uint32_t tail_roots;       // contract once a round's root list is at most this (0: never)
     uint32_t tail_cap;         // tail table slots (a power of two); each entry list holds as many
     ulonglong2* ttab;          // [tail_cap] tail table: (MST, root pair) -> smallest key
@@ -186,6 +188,7 @@ __device__ __forceinline__ void chunk_append_edges(const SweepArgs& a, int which
     }
 }
 
+constexpr uint32_t kNodeChunk = 16;  // nodes a warp claims at a time in the segment walks
 constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0-2)
 constexpr int kWlGroupFlat = 4;   // worklist edges in flight per warp: one root load per endpoint,
 constexpr int kWlGroupHop = 4;    // or two
@@ -563,36 +566,45 @@ __device__ __forceinline__ uint32_t seg_chunk(const SweepArgs& a, uint32_t rp, f
 /// and 2: rounds 0 and 1 flatten every node).  kList builds worklist `which`; kTable
 /// fills the tail table (round 2 as the table round).
 template <int R, bool kList, bool kTable>
-__device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t gw, uint32_t nw, bool act, OfferCache& oc,
+__device__ __forceinline__ bool seg_round(const SweepArgs& a, uint32_t* work, bool act, OfferCache& oc,
                                           TailStage& ts, uint32_t tmask, int which, uint32_t& live_pairs) {
     static_assert(kTailBuf >= 32 + 32 * (kSegGroup - kSegGroup / 2) && kTailBuf >= 32 + 32 * (kSegGroup / 2),
                   "half a group's staged inserts must fit the warp's buffer");
     const unsigned lane = threadIdx.x & 31u;
     bool offered = false;
-    for (uint32_t p = gw; p < a.n; p += nw) {
-        const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
-        if (beg == end) continue;
-        const float cp = act ? __ldg(a.core + static_cast<uint64_t>(p) * kLanes + lane) : 0.0f;
-        const uint32_t rp = act ? root01(a, p, lane, R) : p;
-        unsigned long long seg = kNoKey;
-        for (uint32_t b = beg; b < end; b += 32) {
-            const uint32_t m = min(32u, end - b);
-            uint32_t my_q = 0, my_x = 0, my_y = 0, my_live = 0;
-            float my_w = 0.0f;
-            if (lane < m) {
-                my_x = __ldg(a.eu + b + lane);
-                my_y = __ldg(a.ev + b + lane);
-                my_q = my_x == p ? my_y : my_x;
-                my_w = __ldg(a.ew + b + lane);
+    // warps claim kNodeChunk consecutive nodes at a time from the phase's counter, so a
+    // phase ends when the work does rather than when the slowest fixed share does
+    for (;;) {
+        uint32_t c0 = 0;
+        if (lane == 0) c0 = atomicAdd(work, kNodeChunk);
+        c0 = __shfl_sync(0xFFFFFFFFu, c0, 0);
+        if (c0 >= a.n) break;
+        const uint32_t c1 = min(c0 + kNodeChunk, a.n);
+        for (uint32_t p = c0; p < c1; ++p) {
+            const uint32_t beg = __ldg(a.node_off + p), end = __ldg(a.node_off + p + 1);
+            if (beg == end) continue;
+            const float cp = act ? __ldg(a.core + static_cast<uint64_t>(p) * kLanes + lane) : 0.0f;
+            const uint32_t rp = act ? root01(a, p, lane, R) : p;
+            unsigned long long seg = kNoKey;
+            for (uint32_t b = beg; b < end; b += 32) {
+                const uint32_t m = min(32u, end - b);
+                uint32_t my_q = 0, my_x = 0, my_y = 0, my_live = 0;
+                float my_w = 0.0f;
+                if (lane < m) {
+                    my_x = __ldg(a.eu + b + lane);
+                    my_y = __ldg(a.ev + b + lane);
+                    my_q = my_x == p ? my_y : my_x;
+                    my_w = __ldg(a.ew + b + lane);
+                }
+                const uint32_t pmask =
+                    seg_chunk<R, kList, kTable>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, ts, tmask, live_pairs, my_live);
+                if (kList)
+                    chunk_append_edges(a, which, pmask, make_uint4(b + lane, my_x, my_y, __float_as_uint(my_w)), my_live);
             }
-            const uint32_t pmask =
-                seg_chunk<R, kList, kTable>(a, rp, cp, act, m, b, my_q, my_w, seg, oc, ts, tmask, live_pairs, my_live);
-            if (kList)
-                chunk_append_edges(a, which, pmask, make_uint4(b + lane, my_x, my_y, __float_as_uint(my_w)), my_live);
-        }
-        if (seg != kNoKey) {
-            if (!kTable) offer_min(a, rp, lane, seg);
-            offered = true;
+            if (seg != kNoKey) {
+                if (!kTable) offer_min(a, rp, lane, seg);
+                offered = true;
+            }
         }
     }
     return offered;
@@ -603,7 +615,7 @@ template <int R, bool kList, bool kTable>
 __device__ __forceinline__ bool seg_phase(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, bool act,
                                           OfferCache& oc, TailStage& ts, uint32_t tmask, uint32_t& live_pairs) {
     const int which = (r + 1) & 1;
-    bool offered = seg_round<R, kList, kTable>(a, gw, nw, act, oc, ts, tmask, which, live_pairs);
+    bool offered = seg_round<R, kList, kTable>(a, a.ctr + 11 + (r & 1), act, oc, ts, tmask, which, live_pairs);
     for (uint32_t i = a.e_knn + gw; i < a.E; i += nw) {
         const bool o = bridge_lanes<kList, kTable>(a, i, __ldg(a.eu + i), __ldg(a.ev + i), __ldg(a.ew + i), r, act, oc,
                                                    ts, tmask, which);
@@ -799,6 +811,9 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 tail_ok = false;
                 uint32_t again = 0;
                 if (r == 2) {
+                    // the walk's node counter starts again
+                    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctr[11 + par] = 0;
+                    if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
                     seg_phase<1, true, false>(a, r, gw, nw, act, oc, ts, 0u, again);
                 } else if (flat) {
                     wl_round<true, false>(a, r, gw, nw, act, oc, again, 0u, s_stage);
@@ -819,7 +834,12 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
         {
             const uint32_t rc = r == 0 ? a.n : __ldcg(a.ctr + 2 + par);
             const uint32_t* rin = a.rlist + static_cast<uint64_t>(par) * a.n;
-            for (uint32_t base = gw * 32u; base < rc; base += nw * 32u) {
+            // chunks of 32 roots claimed from the phase's counter
+            for (;;) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(a.ctr + 13 + par, 32u);
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= rc) break;
                 const uint32_t m = min(32u, rc - base);
                 const uint32_t my_c = lane < m ? (r == 0 ? base + lane : __ldcg(rin + base + lane)) : 0u;
                 uint32_t keep = 0;  // roots of this chunk that took an offer
@@ -840,11 +860,15 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
             }
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            a.ctr[par] = 0;      // this round's worklist, consumed
-            a.ctr[9 + par] = 0;  // and its tail entries
+            a.ctr[par] = 0;       // this round's worklist, consumed
+            a.ctr[9 + par] = 0;   // and its tail entries
+            a.ctr[11 + par] = 0;  // and phase A's node counter
         }
         if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) tr[2] = global_ns();
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            tr[2] = global_ns();
+            a.ctr[13 + par] = 0;  // phase B's root counter, consumed
+        }
         // ---- flatten.  Step 1 points at its final root every node of the list whose
         // roots phase B may have linked: in rounds 0 and 1 the list phase B walked
         // (every node with an edge, so that is a full flatten), later the frozen root
