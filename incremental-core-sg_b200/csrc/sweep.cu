@@ -188,7 +188,7 @@ __device__ __forceinline__ void chunk_append_edges(const SweepArgs& a, int which
     }
 }
 
-constexpr uint32_t kNodeChunk = 16;  // nodes a warp claims at a time in the segment walks
+constexpr uint32_t kNodeChunk = 8;   // nodes a warp claims at a time in the segment walks
 constexpr int kSegGroup = 6;      // emitted-segment entries in flight per warp (rounds 0-2)
 constexpr int kWlGroupFlat = 4;   // worklist edges in flight per warp: one root load per endpoint,
 constexpr int kWlGroupHop = 4;    // or two
