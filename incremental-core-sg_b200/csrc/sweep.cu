@@ -271,12 +271,13 @@ __device__ __forceinline__ uint32_t tail_slot(unsigned long long k, uint32_t mas
 
 /// Reduce `key` into the entry of tail key `tk`: linear probing from its slot; a slot
 /// already holding tk takes an atomicMin, an empty one is claimed with atomicCAS.  A
-/// probe sequence longer than kTailProbes sets the overflow flag, and the sweep carries
-/// on over its worklist (written in the table round as in any other).
+/// probe sequence longer than `probes` sets the overflow flag: in the table round the
+/// sweep then carries on over its edge worklist; the tail rounds probe the whole table,
+/// which they size above their entry count, so they always find a slot.
 __device__ __forceinline__ void tail_insert(const SweepArgs& a, uint32_t mask, unsigned long long tk,
-                                            unsigned long long key) {
+                                            unsigned long long key, uint32_t probes = kTailProbes) {
     uint32_t s = tail_slot(tk, mask);
-    for (int p = 0; p < kTailProbes; ++p) {
+    for (uint32_t p = 0; p < probes; ++p) {
         unsigned long long* slot = &a.ttab[s].x;
         unsigned long long cur = __ldcg(slot);
         if (cur == kTailEmpty) cur = atomicCAS(slot, kTailEmpty, tk);
@@ -353,6 +354,7 @@ struct TailStage {
 __device__ __forceinline__ void tail_append(const SweepArgs& a, int which, bool keep, ulonglong2 e,
                                             uint32_t* scan) {
     const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    if (!__syncthreads_or(keep)) return;  // block-uniform
     const unsigned km = __ballot_sync(0xFFFFFFFFu, keep);
     if (lane == 0) scan[w] = static_cast<uint32_t>(__popc(km));
     __syncthreads();
@@ -387,10 +389,13 @@ __device__ __forceinline__ unsigned long long group_min_key(unsigned grp, unsign
 __device__ __forceinline__ void offer_grouped(const SweepArgs& a, bool has, uint32_t root, unsigned j,
                                               unsigned long long key) {
     const unsigned lane = threadIdx.x & 31u;
+    if (!__any_sync(0xFFFFFFFFu, has)) return;
     // roots are below 2^27, so (root << 5 | j) never equals a lane's placeholder
     const unsigned long long gk = has ? ((static_cast<unsigned long long>(root) << 5) | j) : (kTailEmpty - lane);
     const unsigned grp = __match_any_sync(0xFFFFFFFFu, gk);
-    const unsigned long long m = group_min_key(grp, key);
+    // the reductions only where some group has two lanes (a reduction over 32 one-lane
+    // groups costs one pass per group)
+    const unsigned long long m = __any_sync(0xFFFFFFFFu, grp != (1u << lane)) ? group_min_key(grp, key) : key;
     if (has && lane == static_cast<unsigned>(__ffs(grp) - 1)) offer_min(a, root, j, m);
 }
 
@@ -414,47 +419,40 @@ __device__ __forceinline__ void tail_compact(const SweepArgs& a, uint32_t slots,
 }
 
 /// Phase A of a tail round: one thread per entry (MST j, roots x < y as of the round
-/// the entry was last kept, the lightest key between them).  The current roots are
-/// read without writing (the chase from a root of an earlier round through the links
-/// made since: tail rounds do not flatten).  An entry whose roots still differ offers
-/// its key to both and is kept, rewritten with them; entries of a warp that now join
-/// the same two components keep only the lightest.
-__device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t& live_pairs, uint32_t* scan) {
+/// the entry was kept, the lightest key between them).  The current roots are read
+/// without writing (the chase from a root of an earlier round through the links made
+/// since: tail rounds do not flatten).  An entry whose roots still differ goes into the
+/// tail table under its current roots (entries of a warp with the same roots reduced to
+/// their lightest first), so the entries that the round's links made parallel collapse
+/// into one; the compacted table then makes the offers and the next entry list.  The
+/// table has more slots than the list has entries, so a probe of the whole table always
+/// finds one.
+__device__ __forceinline__ bool tail_round(const SweepArgs& a, int r, uint32_t gw, uint32_t nw, uint32_t tmask,
+                                           uint32_t& live_pairs) {
     const unsigned lane = threadIdx.x & 31u;
     const int par = r & 1;
     const uint32_t cnt = __ldcg(a.ctr + 9 + par);
     const ulonglong2* in = a.tl + static_cast<uint64_t>(par) * a.tail_cap;
     bool offered = false;
-    // block-uniform trip count (tail_append synchronises the block)
-    for (uint32_t base = blockIdx.x * blockDim.x; base < cnt; base += gridDim.x * blockDim.x) {
-        const uint32_t t = base + threadIdx.x;
+    for (uint32_t base = gw * 32u; base < cnt; base += nw * 32u) {
+        const uint32_t t = base + lane;
         bool keep = false;
         ulonglong2 e = make_ulonglong2(kTailEmpty, kNoKey);
-        unsigned j = 0;
-        uint32_t rx = 0, ry = 0;
         if (t < cnt) {
             e = __ldcg(in + t);
-            j = static_cast<unsigned>(e.x >> 59);
+            const unsigned j = static_cast<unsigned>(e.x >> 59);
             const uint32_t x = static_cast<uint32_t>(e.x >> 32) & ((1u << kTailNodeBits) - 1u);
             const uint32_t y = static_cast<uint32_t>(e.x);
-            rx = root32(a.parent, x, j, a.n, a.status);
-            ry = root32(a.parent, y, j, a.n, a.status);
+            const uint32_t rx = root32(a.parent, x, j, a.n, a.status);
+            const uint32_t ry = root32(a.parent, y, j, a.n, a.status);
             keep = rx != ry;
             if (keep) e.x = tail_key(j, rx, ry);
         }
-        {
-            const unsigned grp = __match_any_sync(0xFFFFFFFFu, keep ? e.x : kTailEmpty - lane);
-            const unsigned long long m = group_min_key(grp, e.y);
-            if (keep) {
-                e.y = m;
-                keep = lane == static_cast<unsigned>(__ffs(grp) - 1);
-            }
-        }
-        offer_grouped(a, keep, rx, j, e.y);
-        offer_grouped(a, keep, ry, j, e.y);
+        const unsigned grp = __match_any_sync(0xFFFFFFFFu, keep ? e.x : kTailEmpty - lane);
+        const unsigned long long m = __any_sync(0xFFFFFFFFu, grp != (1u << lane)) ? group_min_key(grp, e.y) : e.y;
         live_pairs += keep ? 1u : 0u;
         offered = offered || keep;
-        tail_append(a, (r + 1) & 1, keep, e, scan);
+        if (keep && lane == static_cast<unsigned>(__ffs(grp) - 1)) tail_insert(a, tmask, e.x, m, tmask + 1u);
     }
     return offered;
 }
@@ -776,7 +774,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
         } else if (r == 2) {
             offered = seg_phase<1, true, false>(a, r, gw, nw, act, oc, ts, 0u, live_pairs);
         } else if (mode == 2) {
-            offered = tail_round(a, r, live_pairs, s_scan);
+            offered = tail_round(a, r, gw, nw, tmask, live_pairs);
         } else if (mode == 1) {
             offered = flat ? wl_round<true, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage)
                            : wl_round<false, true>(a, r, gw, nw, act, oc, live_pairs, tmask, s_stage);
@@ -827,6 +825,10 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 tail_compact(a, tmask + 1u, nxt, s_scan);
             }
             if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
+        } else if (mode == 2) {
+            // the re-keyed entries: the next list, and the round's offers
+            tail_compact(a, tmask + 1u, nxt, s_scan);
+            if (!grid_barrier(a.bar, a.bar + 1, a.status, a.limit_ns)) return;
         }
         // ---- phase B: every root that took an offer (all nodes in round 0) links
         // along its best edge; the roots that took one form the next round's list
@@ -858,6 +860,15 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                 }
                 chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
             }
+        }
+        if (mode != 0) {
+            // the next round is a tail round: it re-keys its entries through the table,
+            // cleared here for them, at least twice as many slots as entries
+            const uint32_t cn = __ldcg(a.ctr + 9 + nxt);
+            uint32_t slots = 1024;
+            while (slots < a.tail_cap && static_cast<uint64_t>(slots) < 2ull * cn) slots <<= 1;
+            tmask = slots - 1u;
+            for (uint32_t t = gt; t < slots; t += nt) a.ttab[t] = make_ulonglong2(kTailEmpty, kNoKey);
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.ctr[par] = 0;       // this round's worklist, consumed
