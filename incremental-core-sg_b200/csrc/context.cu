@@ -170,6 +170,16 @@ void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes) {
     cudaEventDestroy(ev[1]);
 }
 
+bool copy_d2h_enqueue(Ctx& c, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return false;
+    if (host_pinned(dst)) {
+        CSB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+        return true;
+    }
+    copy_d2h(c, dst, src, bytes);
+    return false;
+}
+
 void copy_d2h(Ctx& c, void* dst, const void* src, size_t bytes) {
     if (!bytes) return;
     if (host_pinned(dst)) {

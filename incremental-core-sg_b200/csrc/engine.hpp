@@ -263,6 +263,10 @@ void scan_reserve(Ctx& c, uint64_t n);
 // host <-> device through the context's pinned staging (context.cu)
 void copy_h2d(Ctx& c, void* dst, const void* src, size_t bytes);
 void copy_d2h(Ctx& c, void* dst, const void* src, size_t bytes);
+/// Device -> page-locked host memory enqueued on the context stream without waiting
+/// (true: the caller synchronises the stream before reading dst); any other host
+/// memory is copied through the staging at once (false).
+bool copy_d2h_enqueue(Ctx& c, void* dst, const void* src, size_t bytes);
 
 /// Run `f` for a C entry point: lock the context, bind its device, translate
 /// exceptions into a status plus the context's last error.

@@ -1611,14 +1611,36 @@ cs_status cs_extract_sweep(cs_graph* gp, const uint32_t* mpts, uint32_t K, cs_ed
     return guarded(g ? g->ctx : nullptr, [&] {
         CSB_REQUIRE(mpts != nullptr, "cs_extract_sweep: null mpts");
         sweep_run(*g, mpts, K, out_labels != nullptr, nullptr);
+        Ctx& c = *g->ctx;
         const uint64_t cap = g->n ? g->n - 1 : 0;
-        for (uint32_t j = 0; j < K; ++j) {
-            MstHost r;
-            sweep_fetch(*g, j, out_edges ? out_edges + j * cap : nullptr,
-                        out_labels ? out_labels + static_cast<uint64_t>(j) * g->n : nullptr, &r);
-            if (out_nedges) out_nedges[j] = r.nedges;
-            if (out_ncomp) out_ncomp[j] = r.ncomp;
-            if (out_weight) out_weight[j] = r.weight;
+        // per pass: every tree's edge count and weight bins in one read; then each tree
+        // with its labels, waited for before the next (a deeper queue of copies on the
+        // context stream made other contexts' small reads, taken while they hold the
+        // device's sweep turn, wait behind hundreds of MB)
+        uint32_t base = 0;
+        for (SweepPlan* p = g->plan; p; base += p->K, p = p->next) {
+            std::vector<unsigned long long> cnt(p->K);
+            std::vector<uint64_t> bins(static_cast<size_t>(p->K) * 256);
+            CSB_CUDA(cudaMemcpyAsync(cnt.data(), p->counts.p, p->K * 8ull, cudaMemcpyDeviceToHost, c.stream));
+            CSB_CUDA(cudaMemcpyAsync(bins.data(), p->bins.p, bins.size() * 8, cudaMemcpyDeviceToHost, c.stream));
+            CSB_CUDA(cudaStreamSynchronize(c.stream));
+            for (uint32_t jj = 0; jj < p->K; ++jj) {
+                const uint32_t j = base + jj;
+                const uint64_t ne = cnt[jj];
+                if (ne > cap) fail(CS_ERR_STATE, "cs_extract_sweep: the sweep did not complete");
+                if (out_nedges) out_nedges[j] = ne;
+                if (out_ncomp) out_ncomp[j] = static_cast<uint32_t>(p->n - ne);
+                if (out_weight) out_weight[j] = exact_sum_from_bins(bins.data() + static_cast<size_t>(jj) * 256);
+                bool pending = false;
+                if (out_edges && ne)
+                    pending |= copy_d2h_enqueue(c, out_edges + j * cap, p->out.as<cs_edge>() + jj * cap,
+                                                ne * sizeof(cs_edge));
+                if (out_labels && p->n)
+                    pending |= copy_d2h_enqueue(c, out_labels + static_cast<uint64_t>(j) * p->n,
+                                                p->lab.as<uint32_t>() + static_cast<uint64_t>(jj) * p->n,
+                                                static_cast<uint64_t>(p->n) * 4);
+                if (pending) CSB_CUDA(cudaStreamSynchronize(c.stream));
+            }
         }
     });
 }
