@@ -1473,7 +1473,7 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
     }
     if (g.n == 0) fail(CS_ERR_STATE, "sweep: empty graph");
     Ctx& c = *g.ctx;
-    std::lock_guard<std::mutex> device_lock(device_sweep_mutex(c.device));
+    std::unique_lock<std::mutex> device_lock(device_sweep_mutex(c.device));
     graph_build_edges(g);
     uint32_t B = g.sweep_block, F = g.sweep_flatten;
     {
@@ -1516,6 +1516,9 @@ void sweep_run(Graph& g, const uint32_t* mpts, uint32_t K, bool want_labels, flo
     for (SweepPlan* p = g.plan; p; p = p->next) run_pass(g, *p);
     CSB_CUDA(cudaEventRecord(e1, c.stream));
     CSB_CUDA(cudaEventSynchronize(e1));
+    // the device's turn ends with the last kernel: the status and round counts below are
+    // small reads that can wait behind other contexts' copies
+    device_lock.unlock();
     float ms = 0.0f;
     CSB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
