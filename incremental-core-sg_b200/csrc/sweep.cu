@@ -12,12 +12,19 @@
 //     lane j is MST j.  Per-node state is node-major -- parent[v][32], best[v][32] --
 //     so a node's state for all 32 MSTs is one 128/256-byte line and every per-node
 //     access of the warp is coalesced;
-//   * membership of edge i in the 32 trees is one bit-packed word tree[i]; a single
-//     worklist of edges still live in any MST serves all of them, each entry carrying
-//     the edge (index, endpoints, weight) and its live lanes as one bit word;
-//   * rounds 0 and 1 walk each node's emitted segment (the node-major enumeration of
-//     src/knn_graph.cpp:132-200), so the emitter-side atomicMin of every lane is
-//     aggregated over the segment in registers and issued once;
+//   * membership of edge i in the 32 trees is one bit-packed word tree[i]; after round
+//     2, when the tail is off or its table overflowed, a single worklist of edges still
+//     live in any MST serves all of them, each entry carrying the edge (index,
+//     endpoints, weight) and its live lanes as one bit word;
+//   * rounds 0-2 walk each node's emitted segment (the node-major enumeration of
+//     src/knn_graph.cpp:132-200; warps claim a few nodes at a time from a counter), so
+//     the emitter-side atomicMin of every lane is aggregated over the segment in
+//     registers and issued once;
+//   * the contracted tail: once a round's root list is short, the next round (the table
+//     round) reduces every live (edge, MST) pair into a hash table keyed by (MST, root
+//     pair) -- of parallel edges between two components only the lightest can be a tree
+//     edge -- and the compacted entries make its offers; later rounds walk the entries,
+//     one thread each, re-keying them through the table under the current roots;
 //   * between rounds the roots that phase B may have linked are pointed at their
 //     final roots, so a root lookup takes at most two loads; while the live (edge,
 //     MST) pairs outnumber the nodes enough, every node is flattened as well
