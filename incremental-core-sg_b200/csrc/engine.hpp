@@ -122,7 +122,7 @@ struct Graph {
 
     // Scratch kept across calls (grow-only): NN-Descent (knn.cu), the insert path's
     // search and active sets (knn.cu), the bridge selection (bridges.cu).
-    DevBuf knn_scratch[13];
+    DevBuf knn_scratch[14];
     DevBuf insert_scratch[12];
     DevBuf bridge_scratch[23];
 

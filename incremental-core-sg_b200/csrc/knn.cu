@@ -414,133 +414,138 @@ __global__ void __launch_bounds__(kThreads) k_join(const float* __restrict__ pts
 /// the list (LI items per lane) and the chunk are sorted together by a warp bitonic
 /// network of I = 2*LI... elements and the first k kept.  Newcomers carry the new
 /// flag; the ones still listed at the end are the round's updates.
+/// The nodes that took an offer this round (cand.cnt[u] != 0), compacted into a list:
+/// the merge walks them alone instead of a warp for every node of the graph (an insert
+/// round offers to a few hundred thousand nodes of a graph of millions).
+__global__ void k_touched(uint32_t n, const uint32_t* __restrict__ cnt, uint32_t* __restrict__ list,
+                          uint32_t* __restrict__ count) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool has = u < n && cnt[u] != 0;
+    const uint32_t at = warp_append(has, count);  // every lane of the warp calls it
+    if (has) list[at] = u;
+}
+
 template <int LI, int I>
 __global__ void k_merge(uint32_t n, uint32_t k, uint32_t* __restrict__ ids, float* __restrict__ rank,
                         uint8_t* __restrict__ flags, uint32_t* __restrict__ counts, float* __restrict__ thr,
-                        CandStore cand, uint32_t* __restrict__ rnew_cnt, uint32_t* __restrict__ rold_cnt,
+                        CandStore cand, const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count,
                         unsigned long long* __restrict__ updates, uint8_t* __restrict__ changed) {
     static_assert(LI + 1 <= I, "merge layout");
-    const uint32_t u = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    if (u >= n) return;
     const unsigned lane = threadIdx.x & 31u;
-    if (cand.cnt[u] == 0) {  // nothing offered: the list stands; clear the reverse counts
-        if (lane == 0) {
-            rnew_cnt[u] = 0;
-            rold_cnt[u] = 0;
-        }
-        return;
-    }
-    unsigned long long key[I];
-    uint32_t pay[I];  // bit 0: new flag, bit 1: came from an offer
-    const uint32_t c = counts[u];
-    const uint64_t base = static_cast<uint64_t>(u) * k;
-#pragma unroll
-    for (int i = 0; i < I; ++i) {
-        const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
-        if (i < LI && j < c) {
-            key[i] = make_key(rank[base + j], ids[base + j]);
-            pay[i] = flags[base + j] ? 1u : 0u;
-        } else {
-            key[i] = kNoKey;
-            pay[i] = 0;
-        }
-    }
-    const uint32_t offered = cand.cnt[u];
-    const uint32_t nbuf = min(offered, static_cast<uint32_t>(kCap));
-    const bool table_used = offered > static_cast<uint32_t>(kCap);
-    const uint32_t total = nbuf + (table_used ? kSlots : 0);
-    const unsigned long long* bufp = cand.buf + static_cast<uint64_t>(u) * kCap;
-    unsigned long long* tabp = cand.table + static_cast<uint64_t>(u) * kSlots;
-    // k-th key of the current list (element k-1)
-    auto kth_of = [&]() -> unsigned long long {
-        const uint32_t e = k - 1;
-        unsigned long long x = kNoKey;
-#pragma unroll
-        for (int i = 0; i < I; ++i) {
-            const unsigned long long y = __shfl_sync(0xFFFFFFFFu, key[i], e & 31u);
-            if (static_cast<uint32_t>(i) == e / 32u) x = y;
-        }
-        return x;
-    };
-    unsigned long long kth = kth_of();
-    for (uint32_t off = 0; off < total; off += 32) {
-        const uint32_t t = off + lane;
-        unsigned long long ck = kNoKey;
-        if (t < total) {
-            if (t < nbuf) {
-                ck = bufp[t];
-            } else {
-                ck = tabp[t - nbuf];
-                tabp[t - nbuf] = kNoKey;  // the table is reset as it is read
-            }
-        }
-        const uint32_t cid = static_cast<uint32_t>(ck);
-        // kth's rank bits compare like the key's (ids only break exact ties, where a
-        // newcomer does not displace: the reference inserts behind equal distances)
-        bool ok = ck != kNoKey && cid != u && cid < n &&
-                  (kth == kNoKey || static_cast<uint32_t>(ck >> 32) < static_cast<uint32_t>(kth >> 32));
-        // repeated inside the chunk: keep the lowest lane holding the key
-        const unsigned same = __match_any_sync(0xFFFFFFFFu, ck);
-        if (static_cast<int>(lane) != __ffs(same) - 1) ok = false;
-        // already listed
-#pragma unroll
-        for (int i = 0; i < LI; ++i) {
-            const uint32_t lid = static_cast<uint32_t>(key[i]);
-            const bool lv = key[i] != kNoKey;
-            for (int q = 0; q < 32; ++q) {
-                const uint32_t other = __shfl_sync(0xFFFFFFFFu, lid, q);
-                const bool ov = __shfl_sync(0xFFFFFFFFu, lv, q);
-                if (ov && other == cid) ok = false;
-            }
-        }
-        if (!__any_sync(0xFFFFFFFFu, ok)) continue;
-        key[LI] = ok ? ck : kNoKey;
-        pay[LI] = ok ? 3u : 0u;
-#pragma unroll
-        for (int i = LI + 1; i < I; ++i) {
-            key[i] = kNoKey;
-            pay[i] = 0;
-        }
-        warp_bitonic<I>(key, pay);
-        // keep the first k; drop the rest
+    // the nodes that took an offer (k_touched), a warp per node, grid-strided
+    const uint32_t m_list = *list_count;
+    for (uint32_t li = blockIdx.x * kWarps + (threadIdx.x >> 5); li < m_list; li += gridDim.x * kWarps) {
+        const uint32_t u = list[li];
+        unsigned long long key[I];
+        uint32_t pay[I];  // bit 0: new flag, bit 1: came from an offer
+        const uint32_t c = counts[u];
+        const uint64_t base = static_cast<uint64_t>(u) * k;
 #pragma unroll
         for (int i = 0; i < I; ++i) {
             const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
-            if (j >= k) {
+            if (i < LI && j < c) {
+                key[i] = make_key(rank[base + j], ids[base + j]);
+                pay[i] = flags[base + j] ? 1u : 0u;
+            } else {
                 key[i] = kNoKey;
                 pay[i] = 0;
             }
         }
-        kth = kth_of();
-    }
-    uint32_t inserted = 0, cnt = 0;
+        const uint32_t offered = cand.cnt[u];
+        const uint32_t nbuf = min(offered, static_cast<uint32_t>(kCap));
+        const bool table_used = offered > static_cast<uint32_t>(kCap);
+        const uint32_t total = nbuf + (table_used ? kSlots : 0);
+        const unsigned long long* bufp = cand.buf + static_cast<uint64_t>(u) * kCap;
+        unsigned long long* tabp = cand.table + static_cast<uint64_t>(u) * kSlots;
+        // k-th key of the current list (element k-1)
+        auto kth_of = [&]() -> unsigned long long {
+            const uint32_t e = k - 1;
+            unsigned long long x = kNoKey;
 #pragma unroll
-    for (int i = 0; i < LI; ++i) {
-        const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
-        if (j < k) {
-            const bool valid = key[i] != kNoKey;
-            ids[base + j] = valid ? static_cast<uint32_t>(key[i]) : kInvalid;
-            rank[base + j] = valid ? __uint_as_float(static_cast<uint32_t>(key[i] >> 32)) : __int_as_float(0x7f800000);
-            flags[base + j] = valid ? static_cast<uint8_t>(pay[i] & 1u) : 0;
-            cnt += valid;
-            inserted += (valid && (pay[i] & 2u)) ? 1u : 0u;
+            for (int i = 0; i < I; ++i) {
+                const unsigned long long y = __shfl_sync(0xFFFFFFFFu, key[i], e & 31u);
+                if (static_cast<uint32_t>(i) == e / 32u) x = y;
+            }
+            return x;
+        };
+        unsigned long long kth = kth_of();
+        for (uint32_t off = 0; off < total; off += 32) {
+            const uint32_t t = off + lane;
+            unsigned long long ck = kNoKey;
+            if (t < total) {
+                if (t < nbuf) {
+                    ck = bufp[t];
+                } else {
+                    ck = tabp[t - nbuf];
+                    tabp[t - nbuf] = kNoKey;  // the table is reset as it is read
+                }
+            }
+            const uint32_t cid = static_cast<uint32_t>(ck);
+            // kth's rank bits compare like the key's (ids only break exact ties, where a
+            // newcomer does not displace: the reference inserts behind equal distances)
+            bool ok = ck != kNoKey && cid != u && cid < n &&
+                      (kth == kNoKey || static_cast<uint32_t>(ck >> 32) < static_cast<uint32_t>(kth >> 32));
+            // repeated inside the chunk: keep the lowest lane holding the key
+            const unsigned same = __match_any_sync(0xFFFFFFFFu, ck);
+            if (static_cast<int>(lane) != __ffs(same) - 1) ok = false;
+            // already listed
+#pragma unroll
+            for (int i = 0; i < LI; ++i) {
+                const uint32_t lid = static_cast<uint32_t>(key[i]);
+                const bool lv = key[i] != kNoKey;
+                for (int q = 0; q < 32; ++q) {
+                    const uint32_t other = __shfl_sync(0xFFFFFFFFu, lid, q);
+                    const bool ov = __shfl_sync(0xFFFFFFFFu, lv, q);
+                    if (ov && other == cid) ok = false;
+                }
+            }
+            if (!__any_sync(0xFFFFFFFFu, ok)) continue;
+            key[LI] = ok ? ck : kNoKey;
+            pay[LI] = ok ? 3u : 0u;
+#pragma unroll
+            for (int i = LI + 1; i < I; ++i) {
+                key[i] = kNoKey;
+                pay[i] = 0;
+            }
+            warp_bitonic<I>(key, pay);
+            // keep the first k; drop the rest
+#pragma unroll
+            for (int i = 0; i < I; ++i) {
+                const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
+                if (j >= k) {
+                    key[i] = kNoKey;
+                    pay[i] = 0;
+                }
+            }
+            kth = kth_of();
         }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
-        inserted += __shfl_xor_sync(0xFFFFFFFFu, inserted, o);
-    }
-    if (lane == 0) {
-        counts[u] = cnt;
-        thr[u] = (cnt >= k && kth != kNoKey) ? __uint_as_float(static_cast<uint32_t>(kth >> 32))
-                                             : __int_as_float(0x7f800000);
-        cand.cnt[u] = 0;
-        rnew_cnt[u] = 0;
-        rold_cnt[u] = 0;
-        if (inserted && updates) atomicAdd(updates, static_cast<unsigned long long>(inserted));
-        // a newcomer in the list is a change of membership (none got in: the list
-        // holds the same ids); the incremental hubness refresh reads the flag
-        if (inserted) changed[u] = 1;
+        uint32_t inserted = 0, cnt = 0;
+#pragma unroll
+        for (int i = 0; i < LI; ++i) {
+            const uint32_t j = static_cast<uint32_t>(i) * 32u + lane;
+            if (j < k) {
+                const bool valid = key[i] != kNoKey;
+                ids[base + j] = valid ? static_cast<uint32_t>(key[i]) : kInvalid;
+                rank[base + j] = valid ? __uint_as_float(static_cast<uint32_t>(key[i] >> 32)) : __int_as_float(0x7f800000);
+                flags[base + j] = valid ? static_cast<uint8_t>(pay[i] & 1u) : 0;
+                cnt += valid;
+                inserted += (valid && (pay[i] & 2u)) ? 1u : 0u;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+            inserted += __shfl_xor_sync(0xFFFFFFFFu, inserted, o);
+        }
+        if (lane == 0) {
+            counts[u] = cnt;
+            thr[u] = (cnt >= k && kth != kNoKey) ? __uint_as_float(static_cast<uint32_t>(kth >> 32))
+                                                 : __int_as_float(0x7f800000);
+            cand.cnt[u] = 0;
+            if (inserted && updates) atomicAdd(updates, static_cast<unsigned long long>(inserted));
+            // a newcomer in the list is a change of membership (none got in: the list
+            // holds the same ids); the incremental hubness refresh reads the flag
+            if (inserted) changed[u] = 1;
+        }
     }
 }
 
@@ -826,12 +831,13 @@ __global__ void k_rev_keys(const uint32_t* __restrict__ ids, const uint32_t* __r
 
 /// Views of the graph's cached descent scratch (grow-only buffers).
 struct KnnScratch {
-    DevBuf &thr, &cand, &cand_buf, &cand_cnt, &new_s, &old_s, &ns, &nold, &rnew, &rold, &rnew_cnt, &rold_cnt, &counters;
+    DevBuf &thr, &cand, &cand_buf, &cand_cnt, &new_s, &old_s, &ns, &nold, &rnew, &rold, &rnew_cnt, &rold_cnt, &counters,
+        &touched;
     explicit KnnScratch(Graph& g)
         : thr(g.knn_scratch[0]), cand(g.knn_scratch[1]), cand_buf(g.knn_scratch[2]), cand_cnt(g.knn_scratch[3]),
           new_s(g.knn_scratch[4]), old_s(g.knn_scratch[5]), ns(g.knn_scratch[6]), nold(g.knn_scratch[7]),
           rnew(g.knn_scratch[8]), rold(g.knn_scratch[9]), rnew_cnt(g.knn_scratch[10]), rold_cnt(g.knn_scratch[11]),
-          counters(g.knn_scratch[12]) {}
+          counters(g.knn_scratch[12]), touched(g.knn_scratch[13]) {}
 };
 
 /// The node-proportional NN-Descent scratch for `sn` nodes.
@@ -849,6 +855,7 @@ void size_descent_scratch(KnnScratch& s, uint64_t sn) {
     s.rnew_cnt.ensure(sn * 4ull);
     s.rold_cnt.ensure(sn * 4ull);
     s.counters.ensure(64);
+    s.touched.ensure(sn * 4ull);
 }
 
 /// The node-proportional insert scratch (reverse index, active-set marks) for `sn`
@@ -873,19 +880,26 @@ CandStore store_of(KnnScratch& s) {
 
 void launch_merge(Ctx& c, Graph& g, KnnScratch& s, unsigned long long* updates) {
     const uint32_t n = static_cast<uint32_t>(g.n);
-    const unsigned grid = static_cast<unsigned>((n + kWarps - 1) / kWarps);
+    if (n == 0) return;
+    // the nodes that took an offer, then the merge over them (a grid of a few waves)
+    uint32_t* list_count = s.counters.as<uint32_t>() + 4;  // bytes 16-19: after the two 64-bit counters
+    CSB_CUDA(cudaMemsetAsync(list_count, 0, 4, c.stream));
+    k_touched<<<blocks_for(n), kThreads, 0, c.stream>>>(n, s.cand_cnt.as<uint32_t>(), s.touched.as<uint32_t>(),
+                                                         list_count);
+    const unsigned grid = static_cast<unsigned>(
+        std::min<uint64_t>((n + kWarps - 1) / kWarps, static_cast<uint64_t>(std::max(c.sm_count, 1)) * 16));
     if (g.k <= 32) {
         k_merge<1, 2><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
-                                                     store_of(s), s.rnew_cnt.as<uint32_t>(),
-                                                     s.rold_cnt.as<uint32_t>(), updates, g.hub_changed.as<uint8_t>());
+                                                     store_of(s), s.touched.as<uint32_t>(), list_count, updates,
+                                                     g.hub_changed.as<uint8_t>());
     } else {
         k_merge<2, 4><<<grid, kThreads, 0, c.stream>>>(n, g.k, g.ids.as<uint32_t>(), g.dists.as<float>(),
                                                      g.flags.as<uint8_t>(), g.counts.as<uint32_t>(), s.thr.as<float>(),
-                                                     store_of(s), s.rnew_cnt.as<uint32_t>(),
-                                                     s.rold_cnt.as<uint32_t>(), updates, g.hub_changed.as<uint8_t>());
+                                                     store_of(s), s.touched.as<uint32_t>(), list_count, updates,
+                                                     g.hub_changed.as<uint8_t>());
     }
-    count_launch(c);
+    count_launch(c, 2);
 }
 
 }  // namespace
@@ -973,6 +987,9 @@ struct Descent {
         uint32_t done = 0;
         for (uint32_t it = 0; it < iters && m > 0; ++it) {
             CSB_CUDA(cudaMemsetAsync(d_updates, 0, 8, c.stream));
+            // the reverse samples k_sample counts into start empty every round
+            CSB_CUDA(cudaMemsetAsync(s.rnew_cnt.p, 0, n * 4ull, c.stream));
+            CSB_CUDA(cudaMemsetAsync(s.rold_cnt.p, 0, n * 4ull, c.stream));
             k_sample<<<gw, kThreads, 0, c.stream>>>(n, k, smp, g.ids.as<uint32_t>(), g.flags.as<uint8_t>(),
                                                      g.counts.as<uint32_t>(), s.new_s.as<uint32_t>(),
                                                      s.old_s.as<uint32_t>(), s.ns.as<uint32_t>(), s.nold.as<uint32_t>(),
