@@ -861,8 +861,11 @@ __global__ void __launch_bounds__(kMaxBlock, 2) k_sweep(SweepArgs a) {
                     if (has) {
                         *slot = kNoKey;
                         const uint32_t i = static_cast<uint32_t>(key);
-                        const uint32_t bit = 1u << lane;
-                        if (!(atomicOr(a.tree + i, bit) & bit)) unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.n, a.status);
+                        // the tree bit by a reduction (nothing to wait for); both roots of
+                        // an edge they both took call the union, and the second finds
+                        // them united already
+                        atomicOr(a.tree + i, 1u << lane);
+                        unite32(a.parent, __ldg(a.eu + i), __ldg(a.ev + i), lane, a.n, a.status);
                     }
                 }
                 chunk_append(a.rlist, a.ctr + 2, (r + 1) & 1, a.n, keep, my_c);
