@@ -1175,6 +1175,8 @@ struct SweepPlan {
     std::vector<uint32_t> host_mpts;
     const void* key_ptrs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
+    cudaStream_t side = nullptr;                         // the labels' branch of the post graph
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     float last_graph_ms = 0.0f, last_kernel_ms = 0.0f;
     uint32_t last_rounds = 0;
     SweepPlan* next = nullptr;  // the following pass of a sweep with K > 32
@@ -1184,6 +1186,9 @@ struct SweepPlan {
         if (exec_post) cudaGraphExecDestroy(exec_post);
         if (ev_k0) cudaEventDestroy(ev_k0);
         if (ev_k1) cudaEventDestroy(ev_k1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         delete next;
     }
 };
@@ -1277,13 +1282,26 @@ void enqueue_main(Graph& g, SweepPlan& p) {
     count_launch(c);
 }
 
-/// post: labels (optional), tree lists, exact weight bins.
+/// Swaps the context's stream for another until the scope ends.
+struct StreamSwap {
+    Ctx& c;
+    cudaStream_t saved;
+    StreamSwap(Ctx& ctx, cudaStream_t s) : c(ctx), saved(ctx.stream) { c.stream = s; }
+    ~StreamSwap() { c.stream = saved; }
+};
+
+/// post: labels (optional), tree lists, exact weight bins.  The labels and the tree
+/// lists read the same finished forest and write different outputs, so the labels run
+/// on a side stream forked from the context stream and joined back at the end.
 void enqueue_post(Graph& g, SweepPlan& p) {
     Ctx& c = *g.ctx;
     const unsigned wpb = kThreads / 32;
     unsigned long long* nedges = p.counts.as<unsigned long long>();
     unsigned long long* ncomp = nedges + 32;
     if (p.labels) {
+        CSB_CUDA(cudaEventRecord(p.ev_fork, c.stream));
+        CSB_CUDA(cudaStreamWaitEvent(p.side, p.ev_fork, 0));
+        StreamSwap on_side(c, p.side);
         const unsigned gb = static_cast<unsigned>((p.ncn + wpb - 1) / wpb);
         k_lab_count<<<gb, kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n, p.K, p.ncn, p.cc.as<uint32_t>());
         count_launch(c);
@@ -1293,6 +1311,7 @@ void enqueue_post(Graph& g, SweepPlan& p) {
         k_lab_write<<<gb, kThreads, 0, c.stream>>>(p.parent.as<uint32_t>(), p.n, p.K, p.ncn, p.rootlab.as<uint32_t>(),
                                                   p.lab.as<uint32_t>());
         count_launch(c, 2);
+        CSB_CUDA(cudaEventRecord(p.ev_join, c.stream));
     }
     const unsigned ge = static_cast<unsigned>((p.nce + wpb - 1) / wpb);
     k_tree_count<<<ge, kThreads, 0, c.stream>>>(p.tree.as<uint32_t>(), p.E, p.K, p.nce, p.tcnt.as<uint32_t>());
@@ -1305,6 +1324,7 @@ void enqueue_post(Graph& g, SweepPlan& p) {
     dim3 gw(std::max<unsigned>(1, std::min<unsigned>(64, blocks_for(cap))), p.K);
     k_tree_weight<<<gw, kThreads, 0, c.stream>>>(p.out.as<cs_edge>(), cap, nedges, p.bins.as<unsigned long long>());
     count_launch(c, 2);
+    if (p.labels) CSB_CUDA(cudaStreamWaitEvent(c.stream, p.ev_join, 0));
 }
 
 using Enqueue = void (*)(Graph&, SweepPlan&);
@@ -1351,8 +1371,10 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         if (p->exec_post) cudaGraphExecDestroy(p->exec_post);
         if (p->ev_k0) cudaEventDestroy(p->ev_k0);
         if (p->ev_k1) cudaEventDestroy(p->ev_k1);
+        if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+        if (p->ev_join) cudaEventDestroy(p->ev_join);
         p->exec_pre = p->exec_main = p->exec_post = nullptr;
-        p->ev_k0 = p->ev_k1 = nullptr;
+        p->ev_k0 = p->ev_k1 = p->ev_fork = p->ev_join = nullptr;
         delete p->next;
         p->next = nullptr;
     }
@@ -1414,6 +1436,9 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->bins.ensure(static_cast<uint64_t>(K) * 256 * 8);
         CSB_CUDA(cudaEventCreate(&p->ev_k0));
         CSB_CUDA(cudaEventCreate(&p->ev_k1));
+        if (!p->side) CSB_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+        CSB_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+        CSB_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
         int occ = 0;
         CSB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep, static_cast<int>(block), 0));
         if (occ < 1) fail(CS_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
