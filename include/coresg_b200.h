@@ -349,7 +349,7 @@ cs_status cs_set_sweep_shape(cs_graph* g, uint32_t flatten_div, uint32_t block_t
  * (MST, root pair) -> lightest key and the rounds after it walk the table's entries
  * instead of the edges; the trees are the same either way.  tail_div: 0 never,
  * UINT32_MAX the default (4).  table_slots: a cap on the table's slots, a power of two
- * in [2^10, 2^24] (0: the default, min(4 n, |E|) rounded up, at most 2^24); a table
+ * in [2^10, 2^26] (0: the default, min(4 n, |E|) rounded up, at most 2^26); a table
  * that fills past its probe limit leaves the sweep on its edge worklist.  Graphs of
  * 2^27 nodes or more never take the tail.  Plans are recaptured when these change. */
 cs_status cs_set_sweep_tail(cs_graph* g, uint32_t tail_div, uint32_t table_slots);

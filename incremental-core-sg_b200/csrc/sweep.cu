@@ -1413,13 +1413,14 @@ SweepPlan* make_plan(Graph& g, uint32_t K, uint32_t block, uint32_t flatten_div,
         p->bar.ensure(64);
         p->status.ensure(64);
         // the contracted tail: a table of min(4 n, |E|) slots rounded up to a power of
-        // two, at least 2^10 and at most 2^24 (256 MB; a fuller table overflows and the
-        // sweep keeps its worklist), and two entry lists as long; graphs of 2^27 nodes
-        // or more keep the edge worklist to the end
+        // two, at least 2^10 and at most 2^26 (1 GB; the table round holds about 1.6
+        // entries per node, so up to ~20M nodes the table stays under half full, and a
+        // fuller one overflows and the sweep keeps its worklist), and two entry lists as
+        // long; graphs of 2^27 nodes or more keep the edge worklist to the end
         p->tail_div = g.sweep_tail_div;
         p->tail_slots = g.sweep_tail_slots;
         const uint32_t tdiv = g.sweep_tail_div == 0xFFFFFFFFu ? kTailDiv : g.sweep_tail_div;
-        const uint32_t tmax = g.sweep_tail_slots ? g.sweep_tail_slots : (1u << 24);
+        const uint32_t tmax = g.sweep_tail_slots ? g.sweep_tail_slots : (1u << 26);
         p->tail_cap = 1024;
         while (p->tail_cap < std::min<uint64_t>(4 * nc, Ec) && p->tail_cap < tmax) p->tail_cap <<= 1;
         p->tail_roots = (tdiv != 0 && nc < (1ull << kTailNodeBits)) ? static_cast<uint32_t>(n / tdiv) : 0u;
@@ -1761,9 +1762,9 @@ cs_status cs_set_sweep_shape(cs_graph* gp, uint32_t flatten_div, uint32_t block_
 cs_status cs_set_sweep_tail(cs_graph* gp, uint32_t tail_div, uint32_t table_slots) {
     Graph* g = reinterpret_cast<Graph*>(gp);
     return guarded(g ? g->ctx : nullptr, [&] {
-        CSB_REQUIRE(table_slots == 0 || (table_slots >= 1024 && table_slots <= (1u << 24) &&
+        CSB_REQUIRE(table_slots == 0 || (table_slots >= 1024 && table_slots <= (1u << 26) &&
                                          (table_slots & (table_slots - 1)) == 0),
-                    "cs_set_sweep_tail: table_slots must be 0 or a power of two in [2^10, 2^24]");
+                    "cs_set_sweep_tail: table_slots must be 0 or a power of two in [2^10, 2^26]");
         g->sweep_tail_div = tail_div;
         g->sweep_tail_slots = table_slots;
     });
