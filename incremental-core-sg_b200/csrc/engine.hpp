@@ -160,6 +160,11 @@ struct Graph {
     // nodes whose reverse degree changed, a counter; valid after a full pass until the
     // k-NN arrays are replaced.
     bool hub_valid = false;
+    // NN-Descent overflow tables known empty for nodes [0, cand_clean_n) of the buffer at
+    // cand_clean_ptr with cand_clean_bytes (every completed session leaves them so)
+    const void* cand_clean_ptr = nullptr;
+    size_t cand_clean_bytes = 0;
+    uint64_t cand_clean_n = 0;
     uint64_t hub_n = 0;  // nodes scored by the last pass
     DevBuf hub_prev_ids, hub_prev_cnt, hub_changed, hub_rd_dirty, hub_ctr, hub_list;
     void ensure_capacity(uint64_t need, bool keep);

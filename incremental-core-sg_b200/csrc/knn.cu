@@ -928,7 +928,19 @@ struct Descent {
         hub_track(g);  // k_merge flags the nodes whose membership changes
         d_updates = s.counters.as<unsigned long long>();
         d_evals = d_updates + 1;
-        CSB_CUDA(cudaMemsetAsync(s.cand.p, 0xFF, n * 8ull * kSlots, c.stream));
+        // the overflow tables are empty after every completed session (the merge resets
+        // each slot it reads), so only a new buffer, nodes added since, or a session that
+        // did not complete need the memset (at millions of nodes a few GB per insert)
+        {
+            const uint64_t slot_bytes = 8ull * kSlots;
+            uint64_t from = 0;
+            if (g.cand_clean_ptr == s.cand.p && g.cand_clean_bytes == s.cand.bytes)
+                from = std::min<uint64_t>(g.cand_clean_n, n);
+            if (from < n)
+                CSB_CUDA(cudaMemsetAsync(static_cast<char*>(s.cand.p) + from * slot_bytes, 0xFF,
+                                         (n - from) * slot_bytes, c.stream));
+            g.cand_clean_n = 0;  // until finish()
+        }
         CSB_CUDA(cudaMemsetAsync(s.cand_cnt.p, 0, n * 4ull, c.stream));
         CSB_CUDA(cudaMemsetAsync(s.rnew_cnt.p, 0, n * 4ull, c.stream));
         CSB_CUDA(cudaMemsetAsync(s.rold_cnt.p, 0, n * 4ull, c.stream));
@@ -1022,6 +1034,10 @@ struct Descent {
         check_launch(c, "NN-Descent finalize");
         c.sync();
         g.invalidate_edges();
+        // every offer of the session has been merged: the tables are empty again
+        g.cand_clean_ptr = s.cand.p;
+        g.cand_clean_bytes = s.cand.bytes;
+        g.cand_clean_n = n;
     }
 };
 
