@@ -338,7 +338,8 @@ cs_status cs_sweep_timing(cs_graph* g, float* graph_ms, float* kernel_ms);
  * its phase A). */
 cs_status cs_sweep_trace(cs_graph* g, uint64_t* out, uint32_t cap_rounds, uint32_t* out_rounds);
 
-/* Sweep tuning knobs.  flatten_div: after every Boruvka round the roots that were
+/* Sweep tuning knobs (no counterpart in the reference, whose Boruvka has none; the trees
+ * are the same under every setting).  flatten_div: after every Boruvka round the roots that were
  * linked point at their final roots; from round 2 on, every node is flattened too when
  * the round's live (edge, MST) pairs exceed 32 n / flatten_div (0xFFFFFFFF: never);
  * block_threads: 128, 256 or 512.  0 picks the value cached by cs_autotune_sweep for
